@@ -1,0 +1,312 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes front-ends for the two CPU checkers.
+
+* ``Oracle``      - liboracle.so, the plain-C restatement in rzk_oracle.c.
+* ``RefHarness``  - _ref/librzk_ref.so, the reference's own C++ sources compiled in place
+                    (built only where the reference tree exists; the built library
+                    travels with the repository copy).
+
+Only tests/, ``__graft_entry__.smoke()`` and the CPU-baseline leg of bench.py use this
+package, always as the checker.  The product path never imports it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+from renzoku_b200 import scenegen as sg
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "librzk_ref.so")
+REFERENCE_TREE = "/root/reference"
+
+P = ctypes.c_void_p
+I32 = ctypes.c_int32
+U32 = ctypes.c_uint32
+F32 = ctypes.c_float
+
+
+class Counters(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int64) for n in
+                ("rays", "root_tests", "inner_pops", "leaf_tests", "overflows", "pairs",
+                 "culled")]
+
+    def as_dict(self):
+        return {n: int(getattr(self, n)) for n, _ in self._fields_}
+
+
+def build(ref: bool = True) -> None:
+    """Compile liboracle.so and, where the reference tree exists, _ref/librzk_ref.so."""
+    targets = ["oracle"]
+    if ref and os.path.isdir(REFERENCE_TREE):
+        targets.append("ref")
+    subprocess.run(["make", "-s", "-j8", "-C", HERE, *targets], check=True)
+
+
+def _ptr(a: np.ndarray):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+class Oracle:
+    """The C oracle for one scene."""
+
+    _lib = None
+
+    @classmethod
+    def lib(cls):
+        if cls._lib is None:
+            if not os.path.exists(ORACLE_SO):
+                build(ref=False)
+            L = ctypes.CDLL(ORACLE_SO)
+            L.ro_scene_create.restype = P
+            L.ro_scene_create.argtypes = [P]
+            L.ro_scene_destroy.argtypes = [P]
+            for f in ("ro_num_triangles", "ro_num_nodes", "ro_num_lights"):
+                getattr(L, f).restype = I32
+                getattr(L, f).argtypes = [P]
+            L.ro_morton_codes.argtypes = [P, P]
+            L.ro_bvh_dump.argtypes = [P, P, P, P]
+            L.ro_camera_setup.argtypes = [P, P, P, F32, I32, I32, F32, F32, P]
+            L.ro_primary_rays.argtypes = [P, P, P]
+            L.ro_occluded.argtypes = [P, P, P, I32, P, P]
+            L.ro_closest.argtypes = [P, P, P, I32, P, P, P]
+            L.ro_primary.argtypes = [P, P, P, I32]
+            L.ro_gather.argtypes = [P, P, I32, P, I32, I32, F32, F32, I32, P, P, I32, P]
+            L.ro_gather_pairs.argtypes = [P, P, I32, P, I32, I32, F32, P, P]
+            L.ro_incident.argtypes = [P, P, I32, P, I32, I32, F32, P]
+            L.ro_brdf_eval.argtypes = [P, P, P, P, P, I32, P]
+            L.ro_mean_contribution.restype = ctypes.c_double
+            L.ro_mean_contribution.argtypes = [P, P, P, P, I32, P]
+            L.ro_draw_u32.restype = U32
+            L.ro_draw_u32.argtypes = [U32, U32, U32, U32]
+            L.ro_vpl_generate.restype = I32
+            L.ro_vpl_generate.argtypes = [P, U32, I32, I32, P, I32]
+            cls._lib = L
+        return cls._lib
+
+    def __init__(self, scene: sg.Scene):
+        self.scene = scene
+        self._desc = scene.desc()
+        self.h = self.lib().ro_scene_create(ctypes.byref(self._desc))
+        self.n_tris = self.lib().ro_num_triangles(self.h)
+        self.n_nodes = self.lib().ro_num_nodes(self.h)
+
+    def __del__(self):
+        if getattr(self, "h", None) and self._lib is not None:
+            self._lib.ro_scene_destroy(self.h)
+            self.h = None
+
+    def morton_codes(self):
+        out = np.zeros(self.n_tris, np.uint32)
+        self.lib().ro_morton_codes(self.h, _ptr(out))
+        return out
+
+    def bvh(self):
+        codes = np.zeros(self.n_tris, np.uint32)
+        perm = np.zeros(self.n_tris, np.int32)
+        nodes = np.zeros(self.n_nodes, sg.BVH_NODE_DTYPE)
+        self.lib().ro_bvh_dump(self.h, _ptr(codes), _ptr(perm), _ptr(nodes))
+        return codes, perm, nodes
+
+    @staticmethod
+    def camera(spec: sg.CameraSpec) -> np.ndarray:
+        cam = np.zeros(1, sg.CAMERA_DTYPE)
+        f = lambda t: np.asarray(t, np.float32)
+        e, l, u = f(spec.eye), f(spec.lookat), f(spec.up)
+        Oracle.lib().ro_camera_setup(_ptr(e), _ptr(l), _ptr(u), spec.fov, spec.width,
+                                     spec.height, spec.film_w, spec.film_h, _ptr(cam))
+        return cam
+
+    def primary_rays(self, cam: np.ndarray):
+        n = int(cam["width"][0]) * int(cam["height"][0])
+        o = np.zeros((n, 3), np.float32)
+        d = np.zeros((n, 3), np.float32)
+        self.lib().ro_primary_rays(_ptr(cam), _ptr(o), _ptr(d))
+        return o, d
+
+    def primary(self, cam: np.ndarray, threads: int = 8):
+        n = int(cam["width"][0]) * int(cam["height"][0])
+        out = np.zeros(n, sg.RECEIVER_DTYPE)
+        self.lib().ro_primary(self.h, _ptr(cam), _ptr(out), threads)
+        return out
+
+    def occluded(self, p, q):
+        p = np.ascontiguousarray(p, np.float32)
+        q = np.ascontiguousarray(q, np.float32)
+        out = np.zeros(p.shape[0], np.uint8)
+        c = Counters()
+        self.lib().ro_occluded(self.h, _ptr(p), _ptr(q), p.shape[0], _ptr(out), ctypes.byref(c))
+        return out, c.as_dict()
+
+    def closest(self, o, d):
+        o = np.ascontiguousarray(o, np.float32)
+        d = np.ascontiguousarray(d, np.float32)
+        t = np.zeros(o.shape[0], np.float32)
+        rec = np.zeros(o.shape[0], sg.RECEIVER_DTYPE)
+        self.lib().ro_closest(self.h, _ptr(o), _ptr(d), o.shape[0], _ptr(t), _ptr(rec), None)
+        return t, rec
+
+    def gather(self, recv, vpls, clamp_mode, tau, scale=1.0, cull=True, f64=False,
+               threads=8):
+        n = recv.shape[0]
+        out = np.zeros((n, 3), np.float32)
+        out64 = np.zeros((n, 3), np.float64) if f64 else None
+        c = Counters()
+        self.lib().ro_gather(self.h, _ptr(recv), n, _ptr(vpls), vpls.shape[0], clamp_mode,
+                             tau, scale, int(cull), _ptr(out),
+                             _ptr(out64) if f64 else None, threads, ctypes.byref(c))
+        return (out, out64, c.as_dict()) if f64 else (out, c.as_dict())
+
+    def gather_pairs(self, recv, vpls, clamp_mode, tau):
+        n, m = recv.shape[0], vpls.shape[0]
+        rgb = np.zeros((m, n, 3), np.float32)
+        vis = np.zeros((m, n), np.uint8)
+        self.lib().ro_gather_pairs(self.h, _ptr(recv), n, _ptr(vpls), m, clamp_mode, tau,
+                                   _ptr(rgb), _ptr(vis))
+        return rgb, vis
+
+    def incident(self, recv, vpls, clamp_mode, tau):
+        n, m = recv.shape[0], vpls.shape[0]
+        rgb = np.zeros((m, n, 3), np.float32)
+        self.lib().ro_incident(self.h, _ptr(recv), n, _ptr(vpls), m, clamp_mode, tau, _ptr(rgb))
+        return rgb
+
+    def brdf_eval(self, mat, uvn9, wo, wi):
+        n = mat.shape[0]
+        out = np.zeros((n, 3), np.float32)
+        self.lib().ro_brdf_eval(self.h, _ptr(mat), _ptr(uvn9), _ptr(wo), _ptr(wi), n, _ptr(out))
+        return out
+
+    def mean_contribution(self, recv, recv_idx, vpl_idx, vpls):
+        recv_idx = np.ascontiguousarray(recv_idx, np.int32)
+        vpl_idx = np.ascontiguousarray(vpl_idx, np.int32)
+        return float(self.lib().ro_mean_contribution(self.h, _ptr(recv), _ptr(recv_idx),
+                                                     _ptr(vpl_idx), recv_idx.shape[0],
+                                                     _ptr(vpls)))
+
+    def vpl_generate(self, seed, n_particles, max_bounce, cap=None):
+        cap = cap or n_particles * max(1, max_bounce - 1)
+        out = np.zeros(cap, sg.VPL_DTYPE)
+        n = self.lib().ro_vpl_generate(self.h, seed, n_particles, max_bounce, _ptr(out), cap)
+        return out[:min(n, cap)]
+
+    @staticmethod
+    def draw_u32(seed, stream, path, d):
+        return int(Oracle.lib().ro_draw_u32(seed, stream, path, d))
+
+
+class RefHarness:
+    """The reference's own classes for one scene (see ref/ref_harness.cc)."""
+
+    _lib = None
+
+    @staticmethod
+    def available() -> bool:
+        return os.path.exists(REF_SO)
+
+    @classmethod
+    def lib(cls):
+        if cls._lib is None:
+            L = ctypes.CDLL(REF_SO)
+            L.rref_create.restype = P
+            L.rref_create.argtypes = [P, P, U32]
+            L.rref_destroy.argtypes = [P]
+            L.rref_num_triangles.restype = I32
+            L.rref_num_triangles.argtypes = [P]
+            L.rref_num_nodes.restype = I32
+            L.rref_num_nodes.argtypes = [P]
+            L.rref_bvh_dump.restype = I32
+            L.rref_bvh_dump.argtypes = [P, P, P, P, I32]
+            L.rref_camera.argtypes = [P, P]
+            L.rref_occluded.argtypes = [P, P, P, I32, P]
+            L.rref_closest.argtypes = [P, P, P, I32, P, P]
+            L.rref_primary.argtypes = [P, P]
+            L.rref_primary_rays.argtypes = [P, P, P]
+            L.rref_vpl_generate.restype = I32
+            L.rref_vpl_generate.argtypes = [P, U32, I32, I32, P, I32]
+            L.rref_gather.argtypes = [P, P, I32, P, I32, I32, F32, P, P, P]
+            L.rref_incident.argtypes = [P, P, I32, P, I32, I32, F32, P]
+            L.rref_brdf_eval.argtypes = [P, P, P, P, P, I32, P]
+            L.rref_rng_stream.argtypes = [U32, U32, U32]
+            cls._lib = L
+        return cls._lib
+
+    def __init__(self, scene: sg.Scene, seed: int = 2013):
+        self.scene = scene
+        self._desc = scene.desc()
+        self._cam = sg.RefCameraDescC.from_spec(scene.camera)
+        self.h = self.lib().rref_create(ctypes.byref(self._desc), ctypes.byref(self._cam), seed)
+        self.n_tris = self.lib().rref_num_triangles(self.h)
+        self.n_nodes = self.lib().rref_num_nodes(self.h)
+
+    def bvh(self):
+        codes = np.zeros(self.n_tris, np.uint32)
+        perm = np.zeros(self.n_tris, np.int32)
+        nodes = np.zeros(self.n_nodes, sg.BVH_NODE_DTYPE)
+        n = self.lib().rref_bvh_dump(self.h, _ptr(codes), _ptr(perm), _ptr(nodes), self.n_nodes)
+        assert n == self.n_nodes
+        return codes, perm, nodes
+
+    def camera(self):
+        cam = np.zeros(1, sg.CAMERA_DTYPE)
+        self.lib().rref_camera(self.h, _ptr(cam))
+        return cam
+
+    def primary(self):
+        n = self.scene.camera.width * self.scene.camera.height
+        out = np.zeros(n, sg.RECEIVER_DTYPE)
+        self.lib().rref_primary(self.h, _ptr(out))
+        return out
+
+    def primary_rays(self):
+        n = self.scene.camera.width * self.scene.camera.height
+        o = np.zeros((n, 3), np.float32)
+        d = np.zeros((n, 3), np.float32)
+        self.lib().rref_primary_rays(self.h, _ptr(o), _ptr(d))
+        return o, d
+
+    def occluded(self, p, q):
+        p = np.ascontiguousarray(p, np.float32)
+        q = np.ascontiguousarray(q, np.float32)
+        out = np.zeros(p.shape[0], np.uint8)
+        self.lib().rref_occluded(self.h, _ptr(p), _ptr(q), p.shape[0], _ptr(out))
+        return out
+
+    def closest(self, o, d):
+        o = np.ascontiguousarray(o, np.float32)
+        d = np.ascontiguousarray(d, np.float32)
+        t = np.zeros(o.shape[0], np.float32)
+        rec = np.zeros(o.shape[0], sg.RECEIVER_DTYPE)
+        self.lib().rref_closest(self.h, _ptr(o), _ptr(d), o.shape[0], _ptr(t), _ptr(rec))
+        return t, rec
+
+    def vpl_generate(self, seed, n_particles, max_bounce, cap=None):
+        cap = cap or n_particles * max(1, max_bounce - 1) + 16
+        out = np.zeros(cap, sg.VPL_DTYPE)
+        n = self.lib().rref_vpl_generate(self.h, seed, n_particles, max_bounce, _ptr(out), cap)
+        return out[:min(n, cap)]
+
+    def gather(self, recv, vpls, clamp_mode, tau, pairs=False):
+        n, m = recv.shape[0], vpls.shape[0]
+        out = np.zeros((n, 3), np.float32)
+        rgb = np.zeros((m, n, 3), np.float32) if pairs else None
+        vis = np.zeros((m, n), np.uint8) if pairs else None
+        self.lib().rref_gather(self.h, _ptr(recv), n, _ptr(vpls), m, clamp_mode, tau,
+                               _ptr(out), _ptr(rgb) if pairs else None,
+                               _ptr(vis) if pairs else None)
+        return (out, rgb, vis) if pairs else out
+
+    def incident(self, recv, vpls, clamp_mode, tau):
+        n, m = recv.shape[0], vpls.shape[0]
+        rgb = np.zeros((m, n, 3), np.float32)
+        self.lib().rref_incident(self.h, _ptr(recv), n, _ptr(vpls), m, clamp_mode, tau, _ptr(rgb))
+        return rgb
+
+    def brdf_eval(self, mat, uvn9, wo, wi):
+        n = mat.shape[0]
+        out = np.zeros((n, 3), np.float32)
+        self.lib().rref_brdf_eval(self.h, _ptr(mat), _ptr(uvn9), _ptr(wo), _ptr(wi), n, _ptr(out))
+        return out
