@@ -1,0 +1,169 @@
+/*
+ * rzk.h - the C ABI of librzk_cuda.so, the B200 (sm_100a) implementation of Renzoku's
+ * many-light VPL gather path.
+ *
+ * Conventions
+ *   - Every entry point returns an rzk_status (rzk_types.h); nothing throws across the ABI.
+ *   - Pointers named d_* are device pointers, h_* are host pointers; sizes are element
+ *     counts.  `stream` is a cudaStream_t passed as void* (NULL = the legacy default
+ *     stream); every device call is ordered on it and returns without synchronising
+ *     unless its comment says otherwise.
+ *   - Device memory owned by the library lives behind opaque handles (rzk_scene,
+ *     rzk_context).  A context is single-threaded: use one per host thread.
+ *
+ * Each entry point names the reference interface it replaces (file:line in the
+ * reference project).  INTEGRATION.md shows the C++ classes a maintainer adds to the
+ * reference tree to bind them.
+ */
+#ifndef RZK_H_
+#define RZK_H_
+
+#include <stddef.h>
+#include <stdint.h>
+#include "rzk_types.h"
+#include "rzk_scene.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct rzk_context rzk_context;
+typedef struct rzk_scene rzk_scene;
+
+/* Library / context ---------------------------------------------------------------- */
+
+/* Human-readable name of a status code. */
+const char *rzk_status_string(rzk_status s);
+
+/* Creates a context on `device` (cudaSetDevice is called).  The context owns the
+ * gather's reusable scratch buffers and an error word the kernels write on bounded-wait
+ * timeouts.  No reference counterpart (the reference is single-process CPU). */
+rzk_status rzk_context_create(int device, rzk_context **out);
+rzk_status rzk_context_destroy(rzk_context *ctx);
+/* Reads and clears the device error word (RZK_OK when no kernel reported a problem).
+ * Synchronises `stream`. */
+rzk_status rzk_context_check(rzk_context *ctx, void *stream);
+
+/* Aggregate ------------------------------------------------------------------------- */
+
+/* Uploads a scene and builds its device-resident LBVH: replaces
+ * AggregateBvh::AggregateBvh / build (aggregate_bvh.cc:20-240; aggregate_bvh.h:22) and the
+ * scene-side tables of Scene::Scene (scene.cc:26-60, light selection pdf).
+ * The Morton codes, sorted order and BFS node numbering are bit-identical to the
+ * reference's.  Synchronises `stream` (the BFS build reads level sizes back). */
+rzk_status rzk_scene_create(rzk_context *ctx, const rzk_scene_desc *desc, void *stream,
+                            rzk_scene **out);
+rzk_status rzk_scene_destroy(rzk_scene *scene);
+
+/* Triangle, node and level counts and the device bytes the scene holds. */
+rzk_status rzk_scene_info(const rzk_scene *scene, int *n_tris, int *n_nodes, int *n_levels,
+                          size_t *device_bytes);
+
+/* Re-runs the LBVH build on the resident triangles (timing / rebuild after edits).
+ * Same result as rzk_scene_create. Synchronises `stream`. */
+rzk_status rzk_scene_rebuild(rzk_scene *scene, void *stream);
+
+/* Copies the BVH to host buffers in the reference's layout (BvhNode,
+ * aggregate_bvh.h:10-16): sorted Morton codes [n_tris], permutation sorted slot ->
+ * flattened triangle [n_tris], nodes in BFS order [n_nodes].  Any pointer may be NULL.
+ * Synchronises `stream`. */
+rzk_status rzk_bvh_dump(rzk_scene *scene, uint32_t *h_morton_sorted, int32_t *h_perm,
+                        rzk_bvh_node *h_nodes, int cap_nodes, void *stream);
+
+/* Unsorted Morton codes of the flattened triangles (morton.h:98-102), host buffer. */
+rzk_status rzk_morton_codes(rzk_scene *scene, uint32_t *h_codes, void *stream);
+
+/* Aggregate::hit(p, q, tmin, time) for n segments (aggregate.cc:84-90 ->
+ * AggregateBvh::hit any-hit, aggregate_bvh.cc:452-478).  d_out[i] = 1 when occluded. */
+rzk_status rzk_occluded_batch(rzk_scene *scene, const float *d_p, const float *d_q, int n,
+                              uint8_t *d_out, void *stream);
+
+/* Aggregate::hit(ray, tmin, RAY_TMAX, time, HitRecord&) for n rays
+ * (aggregate_bvh.cc:402-448, surface.cc:62-96): d_t[i] = hit distance or -1, and the
+ * hit as a receiver (mat = -1 on a miss). d_recv may be NULL. */
+rzk_status rzk_closest_batch(rzk_scene *scene, const float *d_o, const float *d_d, int n,
+                             float *d_t, rzk_receiver *d_recv, void *stream);
+
+/* One pixel-centre primary hit per pixel: Camera::shoot_ray(i, j) (camera.cc:52-65)
+ * then the closest hit; row-major, row 0 at the top of the image.  `h_cam` is a host
+ * struct (use rzk_camera_setup). d_out has width*height receivers. */
+rzk_status rzk_primary(rzk_scene *scene, const rzk_camera *h_cam, rzk_receiver *d_out,
+                       void *stream);
+
+/* Camera::set_perspective + Camera::focal_length_from_fov + Sensor (camera.cc:23-30,
+ * camera.h:228-230, sensor.h:176-182) computed on the host: the pinhole parameters the
+ * primary-ray kernel consumes. */
+rzk_status rzk_camera_setup(const float eye[3], const float lookat[3], const float up[3],
+                            float fov_deg, int width, int height, float film_w, float film_h,
+                            rzk_camera *h_out);
+
+/* IVplGenerator ----------------------------------------------------------------------- */
+
+/* VplGenerator::spawn (vpl_generator.cc:183-204; generate_vpl 127-181, trace_vpl 43-110;
+ * SubpathGenerator::sample_direct_vertex path.cc:171-334): one thread per light particle,
+ * draw d of particle k from the counter-based stream (seed, 0, k).  VPLs are written to
+ * d_out in the reference's push order (particle-major, bounce-minor), at most `cap`; the
+ * total produced is written to *d_count (device int).  Bounce-0 VPLs are not stored
+ * (vpl_generator.cc:150-151). */
+rzk_status rzk_vpl_generate(rzk_scene *scene, uint32_t seed, int n_particles, int max_bounce,
+                            rzk_vpl *d_out, int cap, int *d_count, void *stream);
+
+/* IVirtualPointLightEvaluator / TransportMatrix ---------------------------------------- */
+
+/* The full gather: d_rgb[r] = scale * sum_j radiance(receiver r, vpl j), where
+ * radiance is VirtualPointLight::gather_point (vpl.cc:661-688) with clamp mode/threshold
+ * (vpl.cc:214-230).  Receivers with mat < 0 get black.  This is the per-pixel sum of
+ * LightTransportMatrix::fill (light_transport_matrix.cc:16-48) without materialising
+ * the matrix, and connect_to_vpl's NONE / POWER_SAMPLING accumulation (vpl.cc:496-520)
+ * over all VPLs.  The sum is deterministic (fixed VPL-chunk order). */
+rzk_status rzk_gather(rzk_context *ctx, rzk_scene *scene, const rzk_receiver *d_recv,
+                      int n_recv, const rzk_vpl *d_vpls, int n_vpl, int clamp_mode, float tau,
+                      float scale, float *d_rgb, void *stream);
+
+/* Number of compiled gather tile configurations (threads per CTA x VPLs per shared-memory
+ * tile); the autotuner searches these. */
+int rzk_gather_variants(void);
+
+/* rzk_gather with an explicit tile configuration: `variant` in [0, rzk_gather_variants())
+ * and `n_chunks` VPL chunks per receiver block (0 = automatic).  All variants give the
+ * same image for the same n_chunks; different n_chunks change only the float summation
+ * order.  n_chunks = 1 sums in exactly the reference's order. */
+rzk_status rzk_gather_cfg(rzk_context *ctx, rzk_scene *scene, const rzk_receiver *d_recv,
+                          int n_recv, const rzk_vpl *d_vpls, int n_vpl, int clamp_mode,
+                          float tau, float scale, float *d_rgb, int variant, int n_chunks,
+                          void *stream);
+
+/* Same computation from host buffers: copies receivers and VPLs to the device, gathers
+ * and copies the image back (the end-to-end drop-in call).  Synchronises `stream`. */
+rzk_status rzk_gather_host(rzk_context *ctx, rzk_scene *scene, const rzk_receiver *h_recv,
+                           int n_recv, const rzk_vpl *h_vpls, int n_vpl, int clamp_mode,
+                           float tau, float scale, float *h_rgb, void *stream);
+
+/* LightTransportMatrix::fill (light_transport_matrix.cc:16-48): every pair's radiance
+ * into a column-major rows x cols MatrixC<Rgb> (matrix_c.h:20-107) d_matrix
+ * [n_vpl][n_recv][3], and optionally its visibility d_vis [n_vpl][n_recv]. */
+rzk_status rzk_gather_matrix(rzk_scene *scene, const rzk_receiver *d_recv, int n_recv,
+                             const rzk_vpl *d_vpls, int n_vpl, int clamp_mode, float tau,
+                             float *d_matrix, uint8_t *d_vis, void *stream);
+
+/* VirtualPointLight::incident_radiance (vpl.cc:411-440) for every pair, column-major
+ * [n_vpl][n_recv][3].  No visibility. */
+rzk_status rzk_incident_matrix(rzk_scene *scene, const rzk_receiver *d_recv, int n_recv,
+                               const rzk_vpl *d_vpls, int n_vpl, int clamp_mode, float tau,
+                               float *d_matrix, void *stream);
+
+/* Mean over n_pairs seeded (receiver, VPL) pairs of RadianceTerms::radiance_no_clamp
+ * .value() (vpl_interface.h:102-116), occluded pairs counted as zero: the base of the
+ * "0.1 x mean contribution" RADIANCE clamp.  Pair k uses receiver
+ * draw(seed,3,k,0) % n_recv and VPL draw(seed,3,k,1) % n_vpl.  *h_mean is written after
+ * `stream` is synchronised. */
+rzk_status rzk_mean_contribution(rzk_context *ctx, rzk_scene *scene,
+                                 const rzk_receiver *d_recv, int n_recv,
+                                 const rzk_vpl *d_vpls, int n_vpl, uint32_t seed,
+                                 int n_pairs, double *h_mean, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RZK_H_ */

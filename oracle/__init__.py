@@ -231,6 +231,7 @@ class RefHarness:
             L.rref_incident.argtypes = [P, P, I32, P, I32, I32, F32, P]
             L.rref_brdf_eval.argtypes = [P, P, P, P, P, I32, P]
             L.rref_rng_stream.argtypes = [U32, U32, U32]
+            L.rref_gather_mt.argtypes = [P, P, I32, P, I32, I32, F32, F32, P, I32]
             cls._lib = L
         return cls._lib
 
@@ -298,6 +299,14 @@ class RefHarness:
                                _ptr(out), _ptr(rgb) if pairs else None,
                                _ptr(vis) if pairs else None)
         return (out, rgb, vis) if pairs else out
+
+    def gather_mt(self, recv, vpls, clamp_mode, tau, scale=1.0, threads=None):
+        """The reference gather on `threads` host threads (all cores by default)."""
+        threads = threads or os.cpu_count() or 1
+        out = np.zeros((recv.shape[0], 3), np.float32)
+        self.lib().rref_gather_mt(self.h, _ptr(recv), recv.shape[0], _ptr(vpls), vpls.shape[0],
+                                  clamp_mode, tau, scale, _ptr(out), threads)
+        return out
 
     def incident(self, recv, vpls, clamp_mode, tau):
         n, m = recv.shape[0], vpls.shape[0]

@@ -26,6 +26,7 @@
 #include <cstring>
 #include <vector>
 #include <string>
+#include <thread>
 
 #include "common.h"
 #include "vec3.h"
@@ -453,6 +454,35 @@ void rref_gather(void *h, const rzk_receiver *recv, int n_recv, const rzk_vpl *v
         }
         put3(out_rgb + 3 * i, sum);
     }
+}
+
+/* The same gather over receivers split across n_threads std::threads (the reference's
+ * AggregateBvh::hit and BRDF evaluation are const and keep no shared state), for timing
+ * the reference CPU path on all host cores.  out_rgb[r] = scale * sum. */
+void rref_gather_mt(void *h, const rzk_receiver *recv, int n_recv, const rzk_vpl *vpls, int n_vpl,
+                    int clamp_mode, float tau, float scale, float *out_rgb, int n_threads) {
+    RefScene *s = (RefScene *)h;
+    std::vector<BrdfPointLight> pls;
+    pls.reserve(n_vpl);
+    for (int j = 0; j < n_vpl; ++j) pls.push_back(to_vpl(s, vpls[j]));
+    if (n_threads < 1) n_threads = 1;
+    auto work = [&](int t) {
+        int r0 = (int)((long long)n_recv * t / n_threads), r1 = (int)((long long)n_recv * (t + 1) / n_threads);
+        for (int i = r0; i < r1; ++i) {
+            Receiver rc = to_receiver(s, recv[i]);
+            LocalGeometry dg(rc);
+            Rgb sum = DefaultRgb::black;
+            for (int j = 0; j < n_vpl; ++j) {
+                bool visible = false;
+                sum += gather_point(s, dg, rc.wo, rc.m, &pls[j], clamp_mode, tau, visible);
+            }
+            put3(out_rgb + 3 * i, sum * scale);
+        }
+    };
+    std::vector<std::thread> th;
+    for (int t = 1; t < n_threads; ++t) th.emplace_back(work, t);
+    work(0);
+    for (auto &x : th) x.join();
 }
 
 /* incident_radiance for every (receiver, VPL) pair, column-major like rref_gather. */

@@ -1,0 +1,113 @@
+// rzk_internal.cuh - library-internal types shared by the .cu files of librzk_cuda.so.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <vector>
+
+#include "../../include/rzk.h"
+#include "rzk_math.cuh"
+
+#define RZK_CUDA_TRY(expr)                                   \
+    do {                                                     \
+        cudaError_t _e = (expr);                             \
+        if (_e != cudaSuccess) {                             \
+            rzk::set_last_cuda_error(_e, #expr, __FILE__, __LINE__); \
+            return _e == cudaErrorMemoryAllocation ? RZK_ERR_NOMEM : RZK_ERR_CUDA; \
+        }                                                    \
+    } while (0)
+
+namespace rzk {
+
+void set_last_cuda_error(cudaError_t e, const char *what, const char *file, int line);
+
+// Device error word bits (written by kernels, read by rzk_context_check).
+enum : uint32_t { ERR_TIMEOUT = 1u, ERR_STACK = 2u, ERR_BOUNDS = 4u };
+
+// Area light as the VPL generator samples it (area_light.cc:27-46, quad.cc:73-87).
+struct DevLight {
+    float4 p0[2], p1[2], p2[2];   // the (one or two) triangles of the light's shape
+    float4 n[2];                  // their facet normals; .w = 1/area
+    float4 basis_n, basis_u;      // Surface::get_basis: larger triangle's n and tangent
+    float4 emit;                  // radiance; .w unused
+    float t0_ratio;
+    int kind, flags, n_tris;
+};
+
+// Everything a kernel needs to trace and shade in one scene (passed by value).
+struct DevScene {
+    const float4 *nodes;      // 2 x float4 per slot, slot = BFS node index + 1
+    const float4 *tri_isect;  // 3 x float4 per sorted triangle (see tri_hit)
+    const float4 *tri_shade;  // 2 x float4 per sorted triangle: {n, surf}, {u, -}
+    const int4 *surf;         // per surface {mat, flags, light, -}
+    const rzk_material *mats;
+    const DevLight *lights;
+    const float *light_pdf;
+    const float *light_cdf;
+    int n_tris, n_nodes, n_mats, n_lights;
+    float tmin;
+    uint32_t *err;            // device error word (context-owned)
+};
+
+struct Scene;
+
+}  // namespace rzk
+
+struct rzk_context {
+    int device = 0;
+    uint32_t *d_err = nullptr;
+    // reusable gather scratch: per-(VPL chunk, receiver) partial sums
+    float *d_partial = nullptr;
+    size_t partial_bytes = 0;
+    // staging for rzk_gather_host
+    void *d_stage = nullptr;
+    size_t stage_bytes = 0;
+    double *d_mean = nullptr;
+};
+
+struct rzk_scene {
+    rzk_context *ctx = nullptr;
+    int n_tris = 0, n_nodes = 0, n_levels = 0, n_surfs = 0, n_mats = 0, n_lights = 0;
+    float tmin = 1e-3f;
+    // original (flattened, input-order) triangles
+    float *d_v = nullptr;        // [n][9]
+    float *d_tp = nullptr;       // [n][3] tangent reference vertex
+    int *d_tri_surf = nullptr;   // [n]
+    float *d_tri_n = nullptr;    // [n][3] facet normal
+    float *d_tri_u = nullptr;    // [n][3] tangent
+    float *d_tri_area = nullptr; // [n]
+    float *d_bmin = nullptr, *d_bmax = nullptr;   // [n][3] triangle boxes
+    // build products
+    uint32_t *d_codes = nullptr, *d_sorted_codes = nullptr;
+    int *d_perm = nullptr;
+    int *d_start = nullptr, *d_end = nullptr, *d_left = nullptr, *d_right = nullptr,
+        *d_level = nullptr;
+    float *d_nbmin = nullptr, *d_nbmax = nullptr;  // [nodes][3]
+    std::vector<int> level_first, level_last;
+    // packed traversal layout
+    float4 *d_nodes = nullptr, *d_tri_isect = nullptr, *d_tri_shade = nullptr;
+    int4 *d_surf = nullptr;
+    rzk_material *d_mats = nullptr;
+    rzk::DevLight *d_lights = nullptr;
+    float *d_light_pdf = nullptr, *d_light_cdf = nullptr;
+    std::vector<int> light_surf;   // host: surface index of each light
+    size_t device_bytes = 0;
+    // scratch for the build (freed after)
+    rzk::DevScene dev() const {
+        rzk::DevScene s;
+        s.nodes = d_nodes; s.tri_isect = d_tri_isect; s.tri_shade = d_tri_shade;
+        s.surf = d_surf; s.mats = d_mats; s.lights = d_lights; s.light_pdf = d_light_pdf;
+        s.light_cdf = d_light_cdf; s.n_tris = n_tris; s.n_nodes = n_nodes; s.n_mats = n_mats;
+        s.n_lights = n_lights; s.tmin = tmin; s.err = ctx ? ctx->d_err : nullptr;
+        return s;
+    }
+};
+
+namespace rzk {
+// rzk_bvh.cu
+rzk_status bvh_build(rzk_scene *s, cudaStream_t st);
+// utilities (rzk_bvh.cu)
+rzk_status exclusive_scan_i32(const int *d_in, int *d_out, int n, int *d_total, void *d_tmp,
+                              size_t tmp_bytes, cudaStream_t st);
+size_t exclusive_scan_tmp_bytes(int n);
+}  // namespace rzk

@@ -1,0 +1,324 @@
+"""ctypes bindings for librzk_cuda.so (include/rzk.h) and the Python-side mirror of the
+reference's plugin interfaces for the VPL gather path.
+
+The classes keep the reference's names and argument meanings so that callers and tests
+read like the reference's own code:
+
+  AggregateCuda           Aggregate / AggregateBvh (aggregate.h:15-91, aggregate_bvh.h:22)
+                          hit(p, q) -> occluded, hit(ray) -> closest hit, BVH dump
+  VplGeneratorCuda        IVplGenerator::spawn (vpl_generator.h:8-21)
+  VirtualPointLightCuda   IVirtualPointLightEvaluator::radiance / incident_radiance
+                          (vpl_interface.h:126-139) batched: gather, transport matrix fill
+  Camera                  Camera::set_perspective / shoot_ray (camera.cc:23-65)
+
+Device buffers are torch CUDA tensors (PyTorch is used for device memory and streams
+only); every computation runs in the CUDA library.  There is no CPU fallback: on a
+machine without the built library or a GPU these classes raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import scenegen as sg
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "librzk_cuda.so")
+
+P = ctypes.c_void_p
+I32 = ctypes.c_int32
+U32 = ctypes.c_uint32
+F32 = ctypes.c_float
+
+# status codes (rzk_types.h)
+OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_TIMEOUT, ERR_STACK, ERR_CAPACITY, ERR_UNSUPPORTED, ERR_BUSY = range(9)
+CLAMP_NONE, CLAMP_FORM_FACTOR, CLAMP_REFLECTIVITY, CLAMP_RADIANCE = range(4)
+
+# every symbol include/rzk.h declares: (name, restype, argtypes)
+SIGNATURES = [
+    ("rzk_status_string", ctypes.c_char_p, [I32]),
+    ("rzk_context_create", I32, [I32, P]),
+    ("rzk_context_destroy", I32, [P]),
+    ("rzk_context_check", I32, [P, P]),
+    ("rzk_scene_create", I32, [P, P, P, P]),
+    ("rzk_scene_destroy", I32, [P]),
+    ("rzk_scene_info", I32, [P, P, P, P, P]),
+    ("rzk_scene_rebuild", I32, [P, P]),
+    ("rzk_bvh_dump", I32, [P, P, P, P, I32, P]),
+    ("rzk_morton_codes", I32, [P, P, P]),
+    ("rzk_occluded_batch", I32, [P, P, P, I32, P, P]),
+    ("rzk_closest_batch", I32, [P, P, P, I32, P, P, P]),
+    ("rzk_primary", I32, [P, P, P, P]),
+    ("rzk_camera_setup", I32, [P, P, P, F32, I32, I32, F32, F32, P]),
+    ("rzk_vpl_generate", I32, [P, U32, I32, I32, P, I32, P, P]),
+    ("rzk_gather", I32, [P, P, P, I32, P, I32, I32, F32, F32, P, P]),
+    ("rzk_gather_variants", I32, []),
+    ("rzk_gather_cfg", I32, [P, P, P, I32, P, I32, I32, F32, F32, P, I32, I32, P]),
+    ("rzk_gather_host", I32, [P, P, P, I32, P, I32, I32, F32, F32, P, P]),
+    ("rzk_gather_matrix", I32, [P, P, I32, P, I32, I32, F32, P, P, P]),
+    ("rzk_incident_matrix", I32, [P, P, I32, P, I32, I32, F32, P, P]),
+    ("rzk_mean_contribution", I32, [P, P, P, I32, P, I32, U32, I32, P, P]),
+]
+
+_LIB = None
+
+
+class RzkError(RuntimeError):
+    def __init__(self, status: int, what: str):
+        self.status = status
+        msg = _LIB.rzk_status_string(status).decode() if _LIB is not None else str(status)
+        super().__init__(f"{what}: {msg} (status {status})")
+
+
+def load(path: str = LIB_PATH):
+    """Load librzk_cuda.so; raises when it has not been built (no fallback)."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(path):
+            raise RuntimeError(f"{path} is missing: run renzoku_b200/build.py (no CPU fallback)")
+        L = ctypes.CDLL(path)
+        for name, res, args in SIGNATURES:
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _LIB = L
+    return _LIB
+
+
+def check(status: int, what: str) -> None:
+    if status != OK:
+        raise RzkError(status, what)
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("renzoku_b200 needs a CUDA device (no CPU fallback)")
+    return torch
+
+
+def _stream_ptr(stream=None):
+    torch = _torch()
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def _dptr(t) -> ctypes.c_void_p:
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def records_to_device(arr: np.ndarray, device="cuda"):
+    """numpy structured records -> contiguous uint8 CUDA tensor of the same bytes."""
+    torch = _torch()
+    raw = np.ascontiguousarray(arr).view(np.uint8).reshape(-1)
+    return torch.from_numpy(raw.copy()).to(device)
+
+
+def records_from_device(t, dtype) -> np.ndarray:
+    return t.detach().cpu().numpy().view(dtype).reshape(-1)
+
+
+class Context:
+    """One device + the library's scratch buffers (rzk_context)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load()
+        self.device = device
+        h = ctypes.c_void_p()
+        check(self.lib.rzk_context_create(device, ctypes.byref(h)), "rzk_context_create")
+        self.h = h
+
+    def check(self, stream=None) -> None:
+        check(self.lib.rzk_context_check(self.h, _stream_ptr(stream)), "device error word")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.rzk_context_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Camera:
+    """Camera::set_perspective + Sensor: the pinhole parameters (rzk_camera)."""
+
+    def __init__(self, spec: sg.CameraSpec):
+        lib = load()
+        self.spec = spec
+        self.rec = np.zeros(1, sg.CAMERA_DTYPE)
+        f = lambda t: np.asarray(t, np.float32)
+        e, l, u = f(spec.eye), f(spec.lookat), f(spec.up)
+        check(lib.rzk_camera_setup(e.ctypes.data, l.ctypes.data, u.ctypes.data, spec.fov,
+                                   spec.width, spec.height, spec.film_w, spec.film_h,
+                                   self.rec.ctypes.data), "rzk_camera_setup")
+
+    @property
+    def n_pixels(self) -> int:
+        return self.spec.width * self.spec.height
+
+
+class AggregateCuda:
+    """Device-resident scene + LBVH; the Aggregate interface (aggregate.h:15-91)."""
+
+    def __init__(self, ctx: Context, scene: sg.Scene, stream=None):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        self.scene = scene
+        self._desc = scene.desc()
+        h = ctypes.c_void_p()
+        check(self.lib.rzk_scene_create(ctx.h, ctypes.byref(self._desc), _stream_ptr(stream),
+                                        ctypes.byref(h)), "rzk_scene_create")
+        self.h = h
+        nt, nn, nl = I32(), I32(), I32()
+        nb = ctypes.c_size_t()
+        check(self.lib.rzk_scene_info(h, ctypes.byref(nt), ctypes.byref(nn), ctypes.byref(nl),
+                                      ctypes.byref(nb)), "rzk_scene_info")
+        self.n_tris, self.n_nodes, self.n_levels, self.device_bytes = nt.value, nn.value, nl.value, nb.value
+        self.tmin = scene.tmin
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.rzk_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def rebuild(self, stream=None):
+        check(self.lib.rzk_scene_rebuild(self.h, _stream_ptr(stream)), "rzk_scene_rebuild")
+
+    def bvh_dump(self):
+        codes = np.zeros(self.n_tris, np.uint32)
+        perm = np.zeros(self.n_tris, np.int32)
+        nodes = np.zeros(self.n_nodes, sg.BVH_NODE_DTYPE)
+        check(self.lib.rzk_bvh_dump(self.h, codes.ctypes.data, perm.ctypes.data, nodes.ctypes.data,
+                                    self.n_nodes, _stream_ptr()), "rzk_bvh_dump")
+        return codes, perm, nodes
+
+    def morton_codes(self):
+        codes = np.zeros(self.n_tris, np.uint32)
+        check(self.lib.rzk_morton_codes(self.h, codes.ctypes.data, _stream_ptr()), "rzk_morton_codes")
+        return codes
+
+    def hit_segments(self, p, q, stream=None):
+        """Aggregate::hit(p, q, tmin, time) for device tensors p, q [n,3] float32: uint8 [n]."""
+        torch = _torch()
+        n = p.shape[0]
+        out = torch.empty(n, dtype=torch.uint8, device=p.device)
+        check(self.lib.rzk_occluded_batch(self.h, _dptr(p), _dptr(q), n, _dptr(out),
+                                          _stream_ptr(stream)), "rzk_occluded_batch")
+        return out
+
+    def hit_rays(self, o, d, stream=None):
+        """Closest hits of rays (o, d): (t [n] float32, receivers [n*96] uint8)."""
+        torch = _torch()
+        n = o.shape[0]
+        t = torch.empty(n, dtype=torch.float32, device=o.device)
+        recv = torch.empty(n * 96, dtype=torch.uint8, device=o.device)
+        check(self.lib.rzk_closest_batch(self.h, _dptr(o), _dptr(d), n, _dptr(t), _dptr(recv),
+                                         _stream_ptr(stream)), "rzk_closest_batch")
+        return t, recv
+
+    def primary(self, camera: Camera, out=None, stream=None):
+        """One pixel-centre primary hit per pixel as receiver records (uint8 tensor)."""
+        torch = _torch()
+        if out is None:
+            out = torch.empty(camera.n_pixels * 96, dtype=torch.uint8, device="cuda")
+        check(self.lib.rzk_primary(self.h, camera.rec.ctypes.data, _dptr(out), _stream_ptr(stream)),
+              "rzk_primary")
+        return out
+
+
+class VplGeneratorCuda:
+    """IVplGenerator::spawn (vpl_generator.h:12-14) on the device."""
+
+    def __init__(self, aggregate: AggregateCuda):
+        self.agg = aggregate
+
+    def spawn(self, seed: int, num_start_particles: int, max_bounce: int, cap: int | None = None,
+              stream=None):
+        torch = _torch()
+        cap = cap or num_start_particles * max(1, max_bounce - 1)
+        out = torch.zeros(cap * 96, dtype=torch.uint8, device="cuda")
+        cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
+        check(self.agg.lib.rzk_vpl_generate(self.agg.h, seed, num_start_particles, max_bounce,
+                                            _dptr(out), cap, _dptr(cnt), _stream_ptr(stream)),
+              "rzk_vpl_generate")
+        n = int(cnt.item())
+        return out[: min(n, cap) * 96], n
+
+
+class VirtualPointLightCuda:
+    """The VPL evaluator (IVirtualPointLightEvaluator, vpl_interface.h:126-139) batched over
+    receivers x VPLs, with the reference's clamp modes (vpl_interface.h:155-162)."""
+
+    def __init__(self, aggregate: AggregateCuda, clamp_mode: int = CLAMP_FORM_FACTOR,
+                 clamp_threshold: float = 1e-3):
+        # VirtualPointLight::VirtualPointLight defaults (vpl.cc:180-202)
+        self.agg = aggregate
+        self.ctx = aggregate.ctx
+        self.clamp_mode = clamp_mode
+        self.clamp_threshold = clamp_threshold
+
+    def gather(self, recv, n_recv, vpls, n_vpl, scale=1.0, out=None, variant=0, n_chunks=0,
+               stream=None):
+        torch = _torch()
+        if out is None:
+            out = torch.empty((n_recv, 3), dtype=torch.float32, device="cuda")
+        check(self.agg.lib.rzk_gather_cfg(self.ctx.h, self.agg.h, _dptr(recv), n_recv, _dptr(vpls),
+                                          n_vpl, self.clamp_mode, self.clamp_threshold, scale,
+                                          _dptr(out), variant, n_chunks, _stream_ptr(stream)),
+              "rzk_gather")
+        return out
+
+    def gather_host(self, recv_np: np.ndarray, vpls_np: np.ndarray, scale=1.0) -> np.ndarray:
+        """End-to-end call on host buffers (pinned or pageable numpy arrays)."""
+        out = np.zeros((recv_np.shape[0], 3), np.float32)
+        check(self.agg.lib.rzk_gather_host(self.ctx.h, self.agg.h, recv_np.ctypes.data,
+                                           recv_np.shape[0], vpls_np.ctypes.data, vpls_np.shape[0],
+                                           self.clamp_mode, self.clamp_threshold, scale,
+                                           out.ctypes.data, _stream_ptr()), "rzk_gather_host")
+        return out
+
+    def fill(self, recv, n_recv, vpls, n_vpl, with_visibility=True, stream=None):
+        """TransportMatrix::fill: column-major [n_vpl, n_recv, 3] matrix (+ visibility)."""
+        torch = _torch()
+        mat = torch.empty((n_vpl, n_recv, 3), dtype=torch.float32, device="cuda")
+        vis = torch.empty((n_vpl, n_recv), dtype=torch.uint8, device="cuda") if with_visibility else None
+        check(self.agg.lib.rzk_gather_matrix(self.agg.h, _dptr(recv), n_recv, _dptr(vpls), n_vpl,
+                                             self.clamp_mode, self.clamp_threshold, _dptr(mat),
+                                             _dptr(vis) if vis is not None else None,
+                                             _stream_ptr(stream)), "rzk_gather_matrix")
+        return mat, vis
+
+    def incident_radiance(self, recv, n_recv, vpls, n_vpl, threshold=None, stream=None):
+        torch = _torch()
+        mat = torch.empty((n_vpl, n_recv, 3), dtype=torch.float32, device="cuda")
+        tau = self.clamp_threshold if threshold is None else threshold
+        check(self.agg.lib.rzk_incident_matrix(self.agg.h, _dptr(recv), n_recv, _dptr(vpls), n_vpl,
+                                               self.clamp_mode, tau, _dptr(mat), _stream_ptr(stream)),
+              "rzk_incident_matrix")
+        return mat
+
+    def mean_contribution(self, recv, n_recv, vpls, n_vpl, seed=0, n_pairs=65536, stream=None):
+        m = ctypes.c_double()
+        check(self.agg.lib.rzk_mean_contribution(self.ctx.h, self.agg.h, _dptr(recv), n_recv,
+                                                 _dptr(vpls), n_vpl, seed, n_pairs, ctypes.byref(m),
+                                                 _stream_ptr(stream)), "rzk_mean_contribution")
+        return m.value
+
+
+def pair_indices(seed: int, n_pairs: int, n_recv: int, n_vpl: int, draw_u32):
+    """The seeded (receiver, VPL) pairs of rzk_mean_contribution, from a draw function."""
+    ri = np.array([draw_u32(seed, 3, k, 0) % n_recv for k in range(n_pairs)], np.int32)
+    vi = np.array([draw_u32(seed, 3, k, 1) % n_vpl for k in range(n_pairs)], np.int32)
+    return ri, vi

@@ -1,0 +1,50 @@
+"""The C-ABI library loads and exports every function include/*.h declares (no GPU calls)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = set()
+    for f in os.listdir(os.path.join(ROOT, "include")):
+        if not f.endswith(".h"):
+            continue
+        src = open(os.path.join(ROOT, "include", f)).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        names.update(re.findall(r"^\s*(?:const\s+)?[A-Za-z_][A-Za-z0-9_]*\s*\*?\s*(rzk_[a-z0-9_]+)\s*\(",
+                                src, flags=re.M))
+    return sorted(names)
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    assert "rzk_gather" in names and "rzk_scene_create" in names and len(names) >= 20
+
+
+def test_library_builds_and_exports_all_symbols():
+    from renzoku_b200 import build, rzk
+    path = build.build()
+    lib = ctypes.CDLL(path)
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+    bound = {n for n, _, _ in rzk.SIGNATURES}
+    assert set(declared_functions()) <= bound | set(), set(declared_functions()) - bound
+
+
+def test_status_strings_without_gpu():
+    from renzoku_b200 import rzk
+    lib = rzk.load()
+    assert lib.rzk_status_string(0) == b"ok"
+    assert b"invalid" in lib.rzk_status_string(1)
+
+
+def test_invalid_arguments_rejected_without_gpu():
+    from renzoku_b200 import rzk
+    lib = rzk.load()
+    assert lib.rzk_scene_create(None, None, None, None) == rzk.ERR_INVALID
+    assert lib.rzk_gather(None, None, None, 0, None, 0, 0, 0.0, 1.0, None, None) == rzk.ERR_INVALID
+    assert lib.rzk_camera_setup(None, None, None, 45.0, 1, 1, 1.0, 1.0, None) == rzk.ERR_INVALID

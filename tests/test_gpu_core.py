@@ -1,0 +1,247 @@
+"""GPU parity tests for the LBVH build, traversal, VPL generation and gather, through the
+C ABI (librzk_cuda.so) against the CPU oracle and the reference's golden outputs."""
+import hashlib
+import os
+
+import numpy as np
+import pytest
+
+from renzoku_b200 import scenegen as sg
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+SCENES = {"room_boxes_32": lambda: sg.room_boxes(32, 32),
+          "room_objects_60": lambda: sg.room_objects(60, 24, 24)}
+TAU = {0: 0.0, 1: 1e-3, 2: 0.05, 3: 0.05}
+
+
+def digest(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+@pytest.fixture(scope="module", params=sorted(SCENES))
+def golden_case(request, ctx, oracle_built):
+    from renzoku_b200 import rzk
+    sc = SCENES[request.param]()
+    g = np.load(os.path.join(GOLDEN, request.param + ".npz"))
+    return request.param, sc, rzk.AggregateCuda(ctx, sc), g
+
+
+def test_bvh_matches_reference(golden_case):
+    name, sc, agg, g = golden_case
+    assert agg.n_tris == int(g["n_tris"]) and agg.n_nodes == int(g["n_nodes"])
+    codes, perm, nodes = agg.bvh_dump()
+    assert np.array_equal(codes, g["codes"])
+    assert np.array_equal(perm, g["perm"])
+    assert digest(nodes) == str(g["nodes_sha"])
+
+
+def test_primary_matches_reference(golden_case):
+    import torch
+    from renzoku_b200 import rzk
+    name, sc, agg, g = golden_case
+    cam = rzk.Camera(sc.camera)
+    assert cam.rec.view(np.uint8).tobytes() == g["camera"].tobytes()
+    recv = agg.primary(cam)
+    torch.cuda.synchronize()
+    assert recv.cpu().numpy().tobytes() == g["recv"].tobytes()
+
+
+def test_occlusion_matches_reference(golden_case):
+    import torch
+    name, sc, agg, g = golden_case
+    p = torch.from_numpy(g["seg_p"]).cuda()
+    q = torch.from_numpy(g["seg_q"]).cuda()
+    occ = agg.hit_segments(p, q).cpu().numpy()
+    assert np.array_equal(occ, g["occluded"])
+    agg.ctx.check()
+
+
+def _vpls_close(a, b):
+    """Same paths and bounces; positions and powers equal up to transcendental ulps."""
+    if a.shape != b.shape or not np.array_equal(a["path"], b["path"]) \
+            or not np.array_equal(a["bounce"], b["bounce"]):
+        return False
+    return (np.allclose(a["p"], b["p"], rtol=1e-4, atol=1e-5)
+            and np.allclose(a["contrib"], b["contrib"], rtol=1e-3, atol=1e-6))
+
+
+def test_vpl_generation_matches_reference(golden_case):
+    from renzoku_b200 import rzk
+    name, sc, agg, g = golden_case
+    gen = rzk.VplGeneratorCuda(agg)
+    t, n = gen.spawn(int(g["vpl_seed"]), int(g["vpl_particles"]), int(g["vpl_max_bounce"]))
+    got = rzk.records_from_device(t, sg.VPL_DTYPE)
+    ref = g["vpl"].view(sg.VPL_DTYPE)
+    assert n == ref.shape[0]
+    same = got.view(np.uint8).tobytes() == ref.view(np.uint8).tobytes()
+    # CUDA's cosf / sinf / powf may differ from glibc's by an ulp; the paths must still agree
+    assert same or _vpls_close(got, ref)
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2, 3])
+def test_gather_matches_reference(golden_case, mode):
+    from renzoku_b200 import rzk
+    name, sc, agg, g = golden_case
+    recv = g["recv"].view(sg.RECEIVER_DTYPE)
+    hit = recv[recv["mat"] >= 0]
+    vpls = g["vpl"].view(sg.VPL_DTYPE)[:128]
+    ev = rzk.VirtualPointLightCuda(agg, mode, TAU[mode])
+    dr, dv = rzk.records_to_device(hit), rzk.records_to_device(vpls)
+    ref = g[f"gather_{mode}"]
+    for variant in range(agg.lib.rzk_gather_variants()):
+        img = ev.gather(dr, hit.shape[0], dv, vpls.shape[0], n_chunks=1, variant=variant).cpu().numpy()
+        if name == "room_boxes_32":
+            # Lambertian only: no transcendental on the path, one chunk sums in the
+            # reference's order -> bit-identical image
+            assert np.array_equal(img, ref), (variant, np.abs(img - ref).max())
+        else:
+            rel = np.linalg.norm(img - ref) / max(np.linalg.norm(ref), 1e-30)
+            assert rel < 1e-5, (variant, rel)
+    agg.ctx.check()
+
+
+@pytest.fixture(scope="module")
+def big(ctx, oracle_built):
+    """The scaled scene: ~300k triangles, 2,000 objects, mixed materials."""
+    from oracle import Oracle
+    from renzoku_b200 import rzk
+    sc = sg.room_objects(2000, 128, 128)
+    return sc, rzk.AggregateCuda(ctx, sc), Oracle(sc)
+
+
+def test_bvh_300k_bit_exact(big):
+    sc, agg, o = big
+    assert agg.n_tris == o.n_tris and agg.n_nodes == o.n_nodes
+    a, b = agg.bvh_dump(), o.bvh()
+    for x, y in zip(a, b):
+        assert x.tobytes() == y.tobytes()
+    assert np.array_equal(agg.morton_codes(), o.morton_codes())
+    agg.rebuild()
+    assert agg.bvh_dump()[2].tobytes() == b[2].tobytes()
+
+
+def test_primary_and_closest_300k_bit_exact(big):
+    import torch
+    from oracle import Oracle
+    from renzoku_b200 import rzk
+    sc, agg, o = big
+    cam = rzk.Camera(sc.camera)
+    got = agg.primary(cam).cpu().numpy()
+    ref = o.primary(Oracle.camera(sc.camera))
+    assert got.tobytes() == ref.view(np.uint8).tobytes()
+    rng = np.random.default_rng(3)
+    orig = rng.uniform(0.05, 0.95, (20000, 3)).astype(np.float32)
+    d = rng.normal(size=(20000, 3)).astype(np.float32)
+    t, r = agg.hit_rays(torch.from_numpy(orig).cuda(), torch.from_numpy(d).cuda())
+    t2, r2 = o.closest(orig, d)
+    assert t.cpu().numpy().tobytes() == t2.tobytes()
+    assert r.cpu().numpy().tobytes() == r2.view(np.uint8).tobytes()
+
+
+def test_occlusion_300k_bit_exact(big):
+    import torch
+    sc, agg, o = big
+    rng = np.random.default_rng(4)
+    p = rng.uniform(0.0, 1.0, (200000, 3)).astype(np.float32)
+    q = rng.uniform(0.0, 1.0, (200000, 3)).astype(np.float32)
+    got = agg.hit_segments(torch.from_numpy(p).cuda(), torch.from_numpy(q).cuda()).cpu().numpy()
+    ref, cnt = o.occluded(p, q)
+    assert cnt["overflows"] == 0
+    assert np.array_equal(got, ref)
+    agg.ctx.check()
+
+
+def test_vplgen_300k_paths_agree(big):
+    from renzoku_b200 import rzk
+    sc, agg, o = big
+    t, n = rzk.VplGeneratorCuda(agg).spawn(17, 4000, 6)
+    got = rzk.records_from_device(t, sg.VPL_DTYPE)
+    ref = o.vpl_generate(17, 4000, 6)
+    assert n == len(got)
+    # per particle: the same VPL count and positions, except where a transcendental ulp
+    # flips a branch; at most 1% of particles may differ structurally
+    bad = 0
+    for k in range(4000):
+        a, b = got[got["path"] == k], ref[ref["path"] == k]
+        if len(a) != len(b) or not np.allclose(a["p"], b["p"], rtol=1e-3, atol=1e-4):
+            bad += 1
+    assert bad <= 40, bad
+
+
+def test_gather_300k_against_oracle(big):
+    from oracle import Oracle
+    from renzoku_b200 import rzk
+    sc, agg, o = big
+    cam = rzk.Camera(sc.camera)
+    recv_t = agg.primary(cam)
+    recv = rzk.records_from_device(recv_t, sg.RECEIVER_DTYPE)
+    vpls = o.vpl_generate(23, 600, 4)
+    dv = rzk.records_to_device(vpls)
+    ev = rzk.VirtualPointLightCuda(agg, rzk.CLAMP_RADIANCE, 0.05)
+    img = ev.gather(recv_t, recv.shape[0], dv, vpls.shape[0], scale=1.0 / 600).cpu().numpy()
+    ref32, ref64, cnt = o.gather(recv, vpls, rzk.CLAMP_RADIANCE, 0.05, scale=1.0 / 600, f64=True)
+    rel32 = np.linalg.norm(img - ref32) / np.linalg.norm(ref32)
+    rel64 = np.linalg.norm(img - ref64) / np.linalg.norm(ref64)
+    assert rel32 < 1e-3 and rel64 < 1e-3, (rel32, rel64)
+    # per-pixel: within 1e-3 relative or 1e-6 absolute
+    assert np.all(np.abs(img - ref32) <= 1e-3 * np.abs(ref32) + 1e-6)
+    agg.ctx.check()
+
+
+def test_matrix_fill_and_incident(big):
+    from renzoku_b200 import rzk
+    sc, agg, o = big
+    cam = rzk.Camera(sc.camera)
+    recv_t = agg.primary(cam)
+    recv = rzk.records_from_device(recv_t, sg.RECEIVER_DTYPE)[::37].copy()
+    vpls = o.vpl_generate(29, 100, 3)
+    dr, dv = rzk.records_to_device(recv), rzk.records_to_device(vpls)
+    ev = rzk.VirtualPointLightCuda(agg, rzk.CLAMP_RADIANCE, 0.05)
+    mat, vis = ev.fill(dr, recv.shape[0], dv, vpls.shape[0])
+    rgb, vis_ref = o.gather_pairs(recv, vpls, rzk.CLAMP_RADIANCE, 0.05)
+    assert np.array_equal(vis.cpu().numpy(), vis_ref)
+    assert np.allclose(mat.cpu().numpy(), rgb, rtol=1e-4, atol=1e-7)
+    inc = ev.incident_radiance(dr, recv.shape[0], dv, vpls.shape[0]).cpu().numpy()
+    assert np.allclose(inc, o.incident(recv, vpls, rzk.CLAMP_RADIANCE, 0.05), rtol=1e-4, atol=1e-7)
+
+
+def test_mean_contribution(big):
+    from oracle import Oracle
+    from renzoku_b200 import rzk
+    sc, agg, o = big
+    recv_t = agg.primary(rzk.Camera(sc.camera))
+    recv = rzk.records_from_device(recv_t, sg.RECEIVER_DTYPE)
+    vpls = o.vpl_generate(31, 300, 3)
+    dv = rzk.records_to_device(vpls)
+    ev = rzk.VirtualPointLightCuda(agg)
+    m = ev.mean_contribution(recv_t, recv.shape[0], dv, vpls.shape[0], seed=9, n_pairs=4096)
+    ri, vi = rzk.pair_indices(9, 4096, recv.shape[0], vpls.shape[0], Oracle.draw_u32)
+    m_ref = o.mean_contribution(recv, ri, vi, vpls)
+    assert m > 0 and abs(m - m_ref) <= 1e-4 * m_ref
+
+
+def test_gather_host_matches_device(big):
+    from renzoku_b200 import rzk
+    sc, agg, o = big
+    recv_t = agg.primary(rzk.Camera(sc.camera))
+    recv = rzk.records_from_device(recv_t, sg.RECEIVER_DTYPE)
+    vpls = o.vpl_generate(37, 200, 3)
+    ev = rzk.VirtualPointLightCuda(agg, rzk.CLAMP_RADIANCE, 0.05)
+    a = ev.gather_host(recv, vpls, scale=0.5)
+    b = ev.gather(recv_t, recv.shape[0], rzk.records_to_device(vpls), vpls.shape[0], scale=0.5).cpu().numpy()
+    assert np.array_equal(a, b)
+
+
+def test_empty_inputs(ctx):
+    import torch
+    from renzoku_b200 import rzk
+    sc = sg.room_boxes(8, 8)
+    agg = rzk.AggregateCuda(ctx, sc)
+    ev = rzk.VirtualPointLightCuda(agg, rzk.CLAMP_RADIANCE, 0.05)
+    recv = agg.primary(rzk.Camera(sc.camera))
+    out = ev.gather(recv, 64, torch.zeros(96, dtype=torch.uint8, device="cuda"), 0)
+    assert float(out.abs().sum()) == 0.0
+    e = torch.zeros((0, 3), dtype=torch.float32, device="cuda")
+    assert agg.hit_segments(e, e).numel() == 0
+    ctx.check()
