@@ -141,15 +141,16 @@ def cpu_rate(sc, o, recv, vpls, tau, scale, budget_s: float, threads: int):
         run = lambda r: ref.gather_mt(r, vpls, 3, tau, scale, threads)
     else:
         run = lambda r: o.gather(r, vpls, 3, tau, scale, cull=False, threads=threads)[0]
-    hit = recv[recv["mat"] >= 0]
-    # calibrate on a small slice, then size the sample to the budget
-    cal = hit[:: max(1, hit.shape[0] // 64)][:64]
+    # seeded uniform sample of all shading points (misses included, as on the GPU);
+    # calibrate on a small slice, then size the sample to the time budget
+    order = np.random.default_rng(VPL_SEED + 1).permutation(recv.shape[0])
+    cal = recv[np.sort(order[:64])].copy()
     t0 = time.perf_counter()
     run(cal)
     dt = max(time.perf_counter() - t0, 1e-3)
     per_recv = dt / cal.shape[0]
-    n = int(max(threads, min(hit.shape[0], budget_s / per_recv)))
-    sample = hit[:: max(1, hit.shape[0] // n)][:n].copy()
+    n = int(max(threads, min(recv.shape[0], budget_s / per_recv)))
+    sample = recv[np.sort(order[:n])].copy()
     return kind, sample, run
 
 
@@ -184,7 +185,7 @@ def run_reference(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "config": workload_config(),
             "cpu_baseline": {"value": v, "unit": "evals/s", "cores": threads, "kind": kind,
-                             "sample": f"{sample.shape[0]} evenly spaced shading points x {vpls.shape[0]} VPLs per step"},
+                             "sample": f"{sample.shape[0]} seeded uniformly sampled shading points x {vpls.shape[0]} VPLs per step"},
             "e2e": {"value": v, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -231,7 +232,7 @@ def run_ours(args):
     stream = torch.cuda.current_stream()
 
     def step():
-        ev.gather(recv_t, n_recv, vpl_t, N_VPL, scale=scale, out=out)
+        ev.gather(recv_t, n_recv, vpl_t, N_VPL, scale=scale, out=out, image_width=WIDTH)
 
     for _ in range(args.warmup):
         step()
@@ -275,7 +276,7 @@ def run_ours(args):
     sp = ctypes.c_void_p(stream.cuda_stream)
 
     def e2e_step():
-        rzk.check(lib.rzk_gather_host(ctx.h, agg.h, ctypes.c_void_p(recv_h.data_ptr()), n_recv,
+        rzk.check(lib.rzk_gather_host(ctx.h, agg.h, ctypes.c_void_p(recv_h.data_ptr()), n_recv, WIDTH,
                                       ctypes.c_void_p(vpl_h.data_ptr()), N_VPL, rzk.CLAMP_RADIANCE,
                                       tau, scale, ctypes.c_void_p(img_h.data_ptr()), sp), "gather_host")
 
@@ -301,7 +302,8 @@ def run_ours(args):
         from oracle import Oracle
         o = Oracle(sc)
         recv_np = rzk.records_from_device(recv_t, sg.RECEIVER_DTYPE)
-        samp = recv_np[:: max(1, n_recv // 512)][:512].copy()
+        rng = np.random.default_rng(VPL_SEED)
+        samp = recv_np[np.sort(rng.choice(n_recv, 512, replace=False))].copy()
         _, cnt = o.gather(samp, vpls_np, rzk.CLAMP_RADIANCE, tau, scale, cull=True,
                           threads=os.cpu_count() or 1)
         pairs = samp.shape[0] * N_VPL
@@ -339,7 +341,7 @@ def run_ours(args):
                          "bytes_per_eval": bytes_per_eval,
                          "note": "BVH (~34 MB) and triangles are L2-resident; algorithmic bytes are served mostly from L2"},
             "cpu_baseline": {"value": cpu_v, "unit": "evals/s", "cores": threads, "kind": kind,
-                             "sample": f"{sample.shape[0]} evenly spaced shading points x {N_VPL} VPLs"},
+                             "sample": f"{sample.shape[0]} seeded uniformly sampled shading points x {N_VPL} VPLs"},
             "clocks": clocks,
             "gpu_launches": 2 * len(times),
             "tau": tau, "num_emitted": num_emitted, "bvh_build_s": build_s,

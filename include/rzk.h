@@ -124,20 +124,24 @@ rzk_status rzk_gather(rzk_context *ctx, rzk_scene *scene, const rzk_receiver *d_
  * tile); the autotuner searches these. */
 int rzk_gather_variants(void);
 
-/* rzk_gather with an explicit tile configuration: `variant` in [0, rzk_gather_variants())
- * and `n_chunks` VPL chunks per receiver block (0 = automatic).  All variants give the
- * same image for the same n_chunks; different n_chunks change only the float summation
- * order.  n_chunks = 1 sums in exactly the reference's order. */
+/* rzk_gather with an explicit layout and tile configuration.  image_width > 0 declares
+ * the receivers a row-major image of that width (as rzk_primary writes them): each warp
+ * then takes an 8 x 4 pixel tile, whose shadow rays are more coherent than a 32-pixel
+ * row; 0 = 32 consecutive receivers per warp.  `variant` in [0, rzk_gather_variants()),
+ * `n_chunks` VPL chunks (0 = automatic).  Layout and variant never change the image;
+ * n_chunks changes only the float summation order, and n_chunks = 1 sums in exactly the
+ * reference's order. */
 rzk_status rzk_gather_cfg(rzk_context *ctx, rzk_scene *scene, const rzk_receiver *d_recv,
-                          int n_recv, const rzk_vpl *d_vpls, int n_vpl, int clamp_mode,
-                          float tau, float scale, float *d_rgb, int variant, int n_chunks,
-                          void *stream);
+                          int n_recv, int image_width, const rzk_vpl *d_vpls, int n_vpl,
+                          int clamp_mode, float tau, float scale, float *d_rgb, int variant,
+                          int n_chunks, void *stream);
 
 /* Same computation from host buffers: copies receivers and VPLs to the device, gathers
- * and copies the image back (the end-to-end drop-in call).  Synchronises `stream`. */
+ * and copies the image back (the end-to-end drop-in call).  image_width as in
+ * rzk_gather_cfg.  Synchronises `stream`. */
 rzk_status rzk_gather_host(rzk_context *ctx, rzk_scene *scene, const rzk_receiver *h_recv,
-                           int n_recv, const rzk_vpl *h_vpls, int n_vpl, int clamp_mode,
-                           float tau, float scale, float *h_rgb, void *stream);
+                           int n_recv, int image_width, const rzk_vpl *h_vpls, int n_vpl,
+                           int clamp_mode, float tau, float scale, float *h_rgb, void *stream);
 
 /* LightTransportMatrix::fill (light_transport_matrix.cc:16-48): every pair's radiance
  * into a column-major rows x cols MatrixC<Rgb> (matrix_c.h:20-107) d_matrix

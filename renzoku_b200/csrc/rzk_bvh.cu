@@ -353,6 +353,53 @@ __global__ void pack_tris_kernel(int n, const int *perm, const float *v, const f
     shade[2 * s + 1] = make_float4(tri_u[3 * t], tri_u[3 * t + 1], tri_u[3 * t + 2], 0.0f);
 }
 
+// K6: 4-wide traversal nodes collapsed from the reference tree.  Every inner node on an
+// even BFS level becomes a node whose entries are its children where they are leaves and
+// its grandchildren otherwise; grandchildren inner nodes are again on an even level.  The
+// entries keep the reference's exact boxes, so a triangle is reached through this tree
+// under exactly the same slab tests as through the binary one (every box contains the
+// boxes below it and the rounded slab test is monotone in the bounds).
+// Record: 8 x float4, entry k = {bmin.xyz, code}, {bmax.xyz, 0}; code = node index,
+// -1 - sorted triangle slot for a leaf, or kWideEmpty.
+__global__ void wide_flag_kernel(int n_nodes, const int *left, const int *level, int *flag) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_nodes) return;
+    flag[i] = (left[i] >= 0 && (level[i] & 1) == 0) ? 1 : 0;
+}
+
+__device__ __forceinline__ void wide_entry(float4 *dst, int node, int code, const float *nbmin,
+                                           const float *nbmax) {
+    dst[0] = make_float4(nbmin[3 * node], nbmin[3 * node + 1], nbmin[3 * node + 2], __int_as_float(code));
+    dst[1] = make_float4(nbmax[3 * node], nbmax[3 * node + 1], nbmax[3 * node + 2], 0.0f);
+}
+
+__global__ void wide_fill_kernel(int n_nodes, const int *start, const int *left, const int *right,
+                                 const int *flag, const int *idx, const float *nbmin, const float *nbmax,
+                                 float4 *wide) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_nodes || !flag[i]) return;
+    float4 *rec = wide + 8 * (size_t)idx[i];
+    int k = 0;
+    const int kids[2] = {left[i], right[i]};
+    for (int a = 0; a < 2; ++a) {
+        int c = kids[a];
+        if (left[c] < 0) {
+            wide_entry(rec + 2 * k++, c, -1 - start[c], nbmin, nbmax);
+        } else {
+            const int g2[2] = {left[c], right[c]};
+            for (int b = 0; b < 2; ++b) {
+                int g = g2[b];
+                int code = left[g] < 0 ? -1 - start[g] : idx[g];
+                wide_entry(rec + 2 * k++, g, code, nbmin, nbmax);
+            }
+        }
+    }
+    for (; k < 4; ++k) {
+        rec[2 * k] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(kWideEmpty));
+        rec[2 * k + 1] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+}
+
 template <class T>
 rzk_status dalloc(T **p, size_t count, size_t *acc) {
     if (*p) return RZK_OK;
@@ -397,7 +444,7 @@ rzk_status bvh_build(rzk_scene *s, cudaStream_t st) {
     // build-only scratch
     const int nblocks_sort = (n + kSortTile - 1) / kSortTile;
     const int hist_n = 256 * nblocks_sort;
-    size_t scan_bytes = std::max(exclusive_scan_tmp_bytes(hist_n), exclusive_scan_tmp_bytes(n));
+    size_t scan_bytes = std::max(exclusive_scan_tmp_bytes(hist_n), exclusive_scan_tmp_bytes(cap));
     size_t scratch_bytes = 0;
     auto carve = [&](size_t bytes) { size_t off = scratch_bytes; scratch_bytes += (bytes + 255) & ~(size_t)255; return off; };
     size_t o_keys2 = carve(sizeof(uint32_t) * (size_t)n);
@@ -405,8 +452,8 @@ rzk_status bvh_build(rzk_scene *s, cudaStream_t st) {
     size_t o_hist = carve(sizeof(int) * (size_t)hist_n);
     size_t o_offs = carve(sizeof(int) * (size_t)hist_n);
     size_t o_split = carve(sizeof(int) * (size_t)n);
-    size_t o_flag = carve(sizeof(int) * (size_t)n);
-    size_t o_rank = carve(sizeof(int) * (size_t)n);
+    size_t o_flag = carve(sizeof(int) * (size_t)cap);
+    size_t o_rank = carve(sizeof(int) * (size_t)cap);
     size_t o_box = carve(sizeof(float) * 6 * 1024 + 64);
     size_t o_total = carve(64);
     size_t o_scan = carve(scan_bytes);
@@ -494,6 +541,26 @@ rzk_status bvh_build(rzk_scene *s, cudaStream_t st) {
     pack_tris_kernel<<<grid, TB, 0, st>>>(n, s->d_perm, s->d_v, s->d_tri_n, s->d_tri_u,
                                           s->d_tri_surf, s->d_tri_isect, s->d_tri_shade);
     RZK_CUDA_TRY(cudaGetLastError());
+    // K6: 4-wide traversal nodes
+    {
+        const int gn = (n_nodes + TB - 1) / TB;
+        wide_flag_kernel<<<gn, TB, 0, st>>>(n_nodes, s->d_left, s->d_level, flag);
+        RZK_TRY(exclusive_scan_i32(flag, rank, n_nodes, total, scan_tmp, scan_bytes, st));
+        int n_wide = 0;
+        RZK_CUDA_TRY(cudaMemcpyAsync(&n_wide, total, sizeof(int), cudaMemcpyDeviceToHost, st));
+        RZK_CUDA_TRY(cudaStreamSynchronize(st));
+        if (!s->d_wide || s->n_wide_cap < n_wide) {
+            if (s->d_wide) cudaFree(s->d_wide);
+            s->d_wide = nullptr;
+            RZK_CUDA_TRY(cudaMalloc((void **)&s->d_wide, 8 * sizeof(float4) * (size_t)std::max(1, n_wide)));
+            s->device_bytes += 8 * sizeof(float4) * (size_t)std::max(1, n_wide);
+            s->n_wide_cap = n_wide;
+        }
+        s->n_wide = n_wide;
+        wide_fill_kernel<<<gn, TB, 0, st>>>(n_nodes, s->d_start, s->d_left, s->d_right, flag, rank,
+                                            s->d_nbmin, s->d_nbmax, s->d_wide);
+        RZK_CUDA_TRY(cudaGetLastError());
+    }
     RZK_CUDA_TRY(cudaStreamSynchronize(st));
     return RZK_OK;
 }

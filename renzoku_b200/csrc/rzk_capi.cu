@@ -23,8 +23,8 @@ rzk_status launch_closest(const DevScene &s, const float *o, const float *d, int
                           rzk_receiver *recv, cudaStream_t st);
 rzk_status launch_primary(const DevScene &s, const rzk_camera &cam, rzk_receiver *out, cudaStream_t st);
 rzk_status launch_gather(rzk_context *ctx, const DevScene &s, const rzk_receiver *recv, int n_recv,
-                         const rzk_vpl *vpls, int n_vpl, int mode, float tau, float scale, float *out,
-                         int variant, int n_chunks, cudaStream_t st);
+                         int img_w, const rzk_vpl *vpls, int n_vpl, int mode, float tau, float scale,
+                         float *out, int variant, int n_chunks, cudaStream_t st);
 int gather_variant_count();
 rzk_status launch_matrix(const DevScene &s, const rzk_receiver *recv, int n_recv, const rzk_vpl *vpls,
                          int n_vpl, int mode, float tau, float *mat, uint8_t *vis, bool incident,
@@ -90,6 +90,7 @@ rzk_status rzk_context_destroy(rzk_context *c) {
     if (c->d_err) cudaFree(c->d_err);
     if (c->d_partial) cudaFree(c->d_partial);
     if (c->d_stage) cudaFree(c->d_stage);
+    if (c->d_work) cudaFree(c->d_work);
     delete c;
     return RZK_OK;
 }
@@ -111,7 +112,7 @@ static void free_scene(rzk_scene *s) {
                     s->d_bmin, s->d_bmax, s->d_codes, s->d_sorted_codes, s->d_perm, s->d_start,
                     s->d_end, s->d_left, s->d_right, s->d_level, s->d_nbmin, s->d_nbmax,
                     s->d_nodes, s->d_tri_isect, s->d_tri_shade, s->d_surf, s->d_mats,
-                    s->d_lights, s->d_light_pdf, s->d_light_cdf};
+                    s->d_lights, s->d_light_pdf, s->d_light_cdf, s->d_wide};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     delete s;
@@ -319,24 +320,25 @@ static rzk_status check_gather_args(rzk_context *ctx, rzk_scene *s, const rzk_re
 int rzk_gather_variants(void) { return gather_variant_count(); }
 
 rzk_status rzk_gather_cfg(rzk_context *ctx, rzk_scene *s, const rzk_receiver *d_recv, int n_recv,
-                          const rzk_vpl *d_vpls, int n_vpl, int clamp_mode, float tau, float scale,
-                          float *d_rgb, int variant, int n_chunks, void *stream) {
+                          int image_width, const rzk_vpl *d_vpls, int n_vpl, int clamp_mode, float tau,
+                          float scale, float *d_rgb, int variant, int n_chunks, void *stream) {
     RZK_TRY(check_gather_args(ctx, s, d_recv, n_recv, d_vpls, n_vpl, clamp_mode));
-    if (n_recv > 0 && !d_rgb) return RZK_ERR_INVALID;
-    return launch_gather(ctx, s->dev(), d_recv, n_recv, d_vpls, n_vpl, clamp_mode, tau, scale, d_rgb,
-                         variant, n_chunks, as_stream(stream));
+    if ((n_recv > 0 && !d_rgb) || image_width < 0) return RZK_ERR_INVALID;
+    return launch_gather(ctx, s->dev(), d_recv, n_recv, image_width, d_vpls, n_vpl, clamp_mode, tau, scale,
+                         d_rgb, variant, n_chunks, as_stream(stream));
 }
 
 rzk_status rzk_gather(rzk_context *ctx, rzk_scene *s, const rzk_receiver *d_recv, int n_recv,
                       const rzk_vpl *d_vpls, int n_vpl, int clamp_mode, float tau, float scale,
                       float *d_rgb, void *stream) {
-    return rzk_gather_cfg(ctx, s, d_recv, n_recv, d_vpls, n_vpl, clamp_mode, tau, scale, d_rgb, 0, 0,
+    return rzk_gather_cfg(ctx, s, d_recv, n_recv, 0, d_vpls, n_vpl, clamp_mode, tau, scale, d_rgb, 0, 0,
                           stream);
 }
 
 rzk_status rzk_gather_host(rzk_context *ctx, rzk_scene *s, const rzk_receiver *h_recv, int n_recv,
-                           const rzk_vpl *h_vpls, int n_vpl, int clamp_mode, float tau, float scale,
-                           float *h_rgb, void *stream) {
+                           int image_width, const rzk_vpl *h_vpls, int n_vpl, int clamp_mode, float tau,
+                           float scale, float *h_rgb, void *stream) {
+    if (image_width < 0) return RZK_ERR_INVALID;
     RZK_TRY(check_gather_args(ctx, s, h_recv, n_recv, h_vpls, n_vpl, clamp_mode));
     if (n_recv > 0 && !h_rgb) return RZK_ERR_INVALID;
     cudaStream_t st = as_stream(stream);
@@ -356,7 +358,8 @@ rzk_status rzk_gather_host(rzk_context *ctx, rzk_scene *s, const rzk_receiver *h
     float *d_out = (float *)((char *)d_vpls + ((vb + 255) & ~(size_t)255));
     if (rb) RZK_CUDA_TRY(cudaMemcpyAsync(d_recv, h_recv, rb, cudaMemcpyHostToDevice, st));
     if (vb) RZK_CUDA_TRY(cudaMemcpyAsync(d_vpls, h_vpls, vb, cudaMemcpyHostToDevice, st));
-    RZK_TRY(launch_gather(ctx, s->dev(), d_recv, n_recv, d_vpls, n_vpl, clamp_mode, tau, scale, d_out, 0, 0, st));
+    RZK_TRY(launch_gather(ctx, s->dev(), d_recv, n_recv, image_width, d_vpls, n_vpl, clamp_mode, tau, scale,
+                          d_out, 0, 0, st));
     if (ob) RZK_CUDA_TRY(cudaMemcpyAsync(h_rgb, d_out, ob, cudaMemcpyDeviceToHost, st));
     RZK_CUDA_TRY(cudaStreamSynchronize(st));
     return RZK_OK;

@@ -188,6 +188,467 @@ __global__ void __launch_bounds__(BLOCK) gather_kernel(DevScene s, const rzk_rec
     }
 }
 
+// ---------------------------------------------------------------------------------
+// Warp-packet gather.
+//
+// A warp owns 32 receivers (an 8 x 4 pixel tile of an image, or 32 consecutive
+// receivers) and streams its VPL chunk through its own double-buffered shared-memory
+// tiles: one cp.async.bulk per tile issued by lane 0, completing on the warp's mbarrier,
+// no block-wide barrier.  For each VPL every lane evaluates its pair's shading term; the
+// lanes with a non-zero term then trace their shadow rays together as a packet: one
+// warp-uniform stack in shared memory, each inner-node visit one broadcast 64-byte load
+// of both children, a child pushed when the box test passes for any lane still
+// unoccluded (ballot).  Each lane tests a leaf's triangle only where its own test of that
+// leaf's box passed, so its answer is exactly the reference's any-hit answer: a
+// triangle is reached iff its own box passes, because every inner box is the exact
+// min / max of the boxes below it and the rounded slab test is monotone in the box
+// bounds.  Rays of one warp toward one VPL are coherent (about 20-26 of the 32 lanes
+// trace together, and the union of their paths is 4-15% longer than the longest single
+// path on the 300k-triangle scene), so the packet costs about what the slowest lane
+// costs alone, with one node fetch per step instead of one per lane.
+// Each lane adds its visible terms in VPL order: the sum is formed in the reference's
+// order.
+// ---------------------------------------------------------------------------------
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ bool finite3(Rgb c) {
+    return isfinite(c.r) && isfinite(c.g) && isfinite(c.b);
+}
+
+// shade() with the BRDFs' own early-outs hoisted: where either BRDF returns black
+// (lambertian.cc:63-66, phong.cc:74-77, ward.cc:104-109: the same dot products, the
+// products commute exactly) and G and the power are finite, the pair's term is exactly
+// zero, so the BRDF values and the clamp need not be formed.
+__device__ __forceinline__ Rgb shade_cull(const DevScene &s, const RecvRegs &r, const rzk_material &rm,
+                                          const rzk_vpl &l, int mode, float tau) {
+    V3 q = ld3(l.p);
+    float G = form_factor_abs(r.p, r.ns, q, ld3(l.n));
+    V3 wi = unit(sub(q, r.p));
+    Rgb power = crgb(l.contrib[0], l.contrib[1], l.contrib[2]);
+    if (isfinite(G) && finite3(power)) {
+        if (dot(wi, r.uvn.n) <= ZERO_EPSILON || dot(r.wo, r.uvn.n) <= ZERO_EPSILON)
+            return crgb(0.0f, 0.0f, 0.0f);
+        if (l.mat >= 0) {
+            V3 lnn = ld3(l.nn);
+            if (dot(neg(wi), lnn) <= ZERO_EPSILON || dot(ld3(l.wi), lnn) <= ZERO_EPSILON)
+                return crgb(0.0f, 0.0f, 0.0f);
+        }
+    }
+    Rgb sb = brdf_eval(rm, r.uvn, r.wo, wi);
+    Rgb lb;
+    if (l.mat >= 0) {
+        rzk_material lm = load_material(s.mats + l.mat);
+        Onb lu{ld3(l.u), ld3(l.v), ld3(l.nn)};
+        lb = brdf_eval(lm, lu, ld3(l.wi), neg(wi));
+    } else {
+        lb = crgb(1.0f, 1.0f, 1.0f);
+    }
+    return radiance_terms(power, sb, lb, G, mode, tau);
+}
+
+// Receiver index of a lane: an 8 x 4 tile of a row-major image of width img_w, or 32
+// consecutive receivers when img_w == 0.  -1 outside the receiver range.
+__device__ __forceinline__ int lane_receiver(int gwarp, int lane, int n_recv, int img_w) {
+    if (img_w <= 0) {
+        int ri = gwarp * 32 + lane;
+        return ri < n_recv ? ri : -1;
+    }
+    int tiles_x = (img_w + 7) >> 3;
+    int x = (gwarp % tiles_x) * 8 + (lane & 7);
+    int y = (gwarp / tiles_x) * 4 + (lane >> 3);
+    if (x >= img_w) return -1;
+    long long ri = (long long)y * img_w + x;
+    return ri < n_recv ? (int)ri : -1;
+}
+
+// Packet any-hit for the lanes in `act`; returns the lanes that stay unoccluded.
+__device__ __forceinline__ bool packet_visible(const DevScene &s, const Ray &ray, float tmax, bool act,
+                                               int *stk) {
+    if (s.n_nodes == 0) return act;
+    const float4 lo = __ldg(s.nodes + 2), hi = __ldg(s.nodes + 3);
+    bool hit_root = act && box_hit(lo, hi, ray, s.tmin, tmax);
+    if (!__any_sync(kFull, hit_root)) return act;
+    const int a = __float_as_int(lo.w);
+    if (a < 0) {
+        if (hit_root) {
+            float4 ta, tb, tc;
+            load_tri(s, -1 - a, ta, tb, tc);
+            if (tri_hit<false>(ta, tb, tc, ray, s.tmin, tmax, nullptr, nullptr, nullptr)) act = false;
+        }
+        return act;
+    }
+    // lanes whose root test failed cannot reach any triangle below it
+    bool alive = hit_root;
+    int top = 0;
+    stk[0] = a;
+    bool overflow = false;
+    while (top >= 0) {
+        const int c = stk[top--];
+        const float4 *pn = s.nodes + 2 * (c + 1);
+        const float4 l0 = __ldg(pn), l1 = __ldg(pn + 1), r0 = __ldg(pn + 2), r1 = __ldg(pn + 3);
+        const int al = __float_as_int(l0.w), ar = __float_as_int(r0.w);
+        bool hl = alive && box_hit(l0, l1, ray, s.tmin, tmax);
+        bool hr = alive && box_hit(r0, r1, ray, s.tmin, tmax);
+        if (al < 0 && hl) {
+            float4 ta, tb, tc;
+            load_tri(s, -1 - al, ta, tb, tc);
+            if (tri_hit<false>(ta, tb, tc, ray, s.tmin, tmax, nullptr, nullptr, nullptr)) alive = false;
+        }
+        if (ar < 0 && hr && alive) {
+            float4 ta, tb, tc;
+            load_tri(s, -1 - ar, ta, tb, tc);
+            if (tri_hit<false>(ta, tb, tc, ray, s.tmin, tmax, nullptr, nullptr, nullptr)) alive = false;
+        }
+        if (!alive) act = false;
+        // push order as the reference: left first, so the right child is visited next
+        if (al >= 0 && __any_sync(kFull, hl && alive)) {
+            if (top < STACK_CAP - 1) stk[++top] = al; else overflow = true;
+        }
+        if (ar >= 0 && __any_sync(kFull, hr && alive)) {
+            if (top < STACK_CAP - 1) stk[++top] = ar; else overflow = true;
+        }
+        if (!__any_sync(kFull, alive)) break;
+    }
+    if (overflow && s.err) atomicOr(s.err, ERR_STACK);
+    return act;
+}
+
+// Packet any-hit over the 4-wide tree: per step one broadcast 128-byte node load, four
+// independent box tests per lane, leaf triangles tested where the lane's own leaf-box
+// test passed, inner entries pushed when any unoccluded lane passed them.
+__device__ __forceinline__ bool packet_visible_wide(const DevScene &s, const Ray &ray, float tmax, bool act,
+                                                    int *stk) {
+    if (s.n_nodes == 0) return act;
+    const float4 lo = __ldg(s.nodes + 2), hi = __ldg(s.nodes + 3);
+    bool alive = act && box_hit(lo, hi, ray, s.tmin, tmax);
+    if (!__any_sync(kFull, alive)) return act;
+    const int a = __float_as_int(lo.w);
+    if (a < 0) {
+        if (alive) {
+            float4 ta, tb, tc;
+            load_tri(s, -1 - a, ta, tb, tc);
+            if (tri_hit<false>(ta, tb, tc, ray, s.tmin, tmax, nullptr, nullptr, nullptr)) act = false;
+        }
+        return act;
+    }
+    int top = 0;
+    stk[0] = 0;
+    bool overflow = false;
+    while (top >= 0) {
+        const float4 *pn = s.wide + 8 * stk[top--];
+        float4 e0[4], e1[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) { e0[k] = __ldg(pn + 2 * k); e1[k] = __ldg(pn + 2 * k + 1); }
+        bool h[4];
+        int code[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            code[k] = __float_as_int(e0[k].w);
+            h[k] = alive && code[k] != kWideEmpty && box_hit(e0[k], e1[k], ray, s.tmin, tmax);
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (code[k] < 0 && h[k] && alive) {
+                float4 ta, tb, tc;
+                load_tri(s, -1 - code[k], ta, tb, tc);
+                if (tri_hit<false>(ta, tb, tc, ray, s.tmin, tmax, nullptr, nullptr, nullptr)) alive = false;
+            }
+        }
+        if (!alive) act = false;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (code[k] >= 0 && code[k] != kWideEmpty && __any_sync(kFull, h[k] && alive)) {
+                if (top < STACK_CAP - 1) stk[++top] = code[k]; else overflow = true;
+            }
+        }
+        if (!__any_sync(kFull, alive)) break;
+    }
+    if (overflow && s.err) atomicOr(s.err, ERR_STACK);
+    return act;
+}
+
+template <int WARPS, int TILE, bool WIDE>
+__global__ void __launch_bounds__(WARPS * 32) gather_packet_kernel(DevScene s, const rzk_receiver *recv,
+                                                                   int n_recv, int img_w,
+                                                                   const rzk_vpl *vpls, int n_vpl,
+                                                                   int chunk_len, int mode, float tau,
+                                                                   float *partial) {
+    __shared__ __align__(128) rzk_vpl tiles[WARPS][2][TILE];
+    __shared__ __align__(8) uint64_t bar[WARPS][2];
+    __shared__ int stacks[WARPS][STACK_CAP];
+
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int ri = lane_receiver(blockIdx.x * WARPS + w, lane, n_recv, img_w);
+    const int chunk = blockIdx.y;
+    const int j0 = chunk * chunk_len;
+    const int j1 = min(n_vpl, j0 + chunk_len);
+    const int n_tiles = j1 > j0 ? (j1 - j0 + TILE - 1) / TILE : 0;
+
+    RecvRegs r;
+    r.p = mk(0.0f, 0.0f, 0.0f);   // lanes without a receiver still form (unused) rays
+    bool active = false;
+    rzk_material rm;
+    if (ri >= 0) {
+        r = load_receiver(recv + ri);
+        active = r.mat >= 0;
+        if (active) rm = load_material(s.mats + r.mat);
+    }
+    uint64_t *mb = bar[w];
+    rzk_vpl(*tl)[TILE] = tiles[w];
+    int *stk = stacks[w];
+
+    if (lane == 0) {
+        mbar_init(&mb[0], 1);
+        mbar_init(&mb[1], 1);
+        fence_barrier_init();
+        if (n_tiles > 0) {
+            int cnt = min(TILE, j1 - j0);
+            mbar_expect_tx(&mb[0], cnt * (uint32_t)sizeof(rzk_vpl));
+            bulk_g2s(&tl[0][0], vpls + j0, cnt * (uint32_t)sizeof(rzk_vpl), &mb[0]);
+        }
+    }
+    __syncwarp();
+
+    Rgb sum = crgb(0.0f, 0.0f, 0.0f);
+    for (int k = 0; k < n_tiles; ++k) {
+        const int buf = k & 1;
+        if (lane == 0 && k + 1 < n_tiles) {
+            int jn = j0 + (k + 1) * TILE;
+            int cnt = min(TILE, j1 - jn);
+            fence_proxy_async();
+            mbar_expect_tx(&mb[buf ^ 1], cnt * (uint32_t)sizeof(rzk_vpl));
+            bulk_g2s(&tl[buf ^ 1][0], vpls + jn, cnt * (uint32_t)sizeof(rzk_vpl), &mb[buf ^ 1]);
+        }
+        bool ok = mbar_wait_bounded(&mb[buf], (k >> 1) & 1, lane == 0 ? s.err : nullptr);
+        if (__any_sync(kFull, !ok)) break;
+        const rzk_vpl *tile = tl[buf];
+        const int cnt = min(TILE, j1 - (j0 + k * TILE));
+        for (int v = 0; v < cnt; ++v) {
+            const rzk_vpl &l = tile[v];
+            Rgb L = crgb(0.0f, 0.0f, 0.0f);
+            bool act = false;
+            if (active) {
+                L = shade_cull(s, r, rm, l, mode, tau);
+                act = !cblack(L);
+            }
+            if (!__any_sync(kFull, act)) continue;
+            V3 q = ld3(l.p);
+            Ray ray = make_ray(r.p, sub(q, r.p));
+            float tmax = len(sub(q, r.p)) - s.tmin;
+            bool vis = WIDE ? packet_visible_wide(s, ray, tmax, act, stk) : packet_visible(s, ray, tmax, act, stk);
+            if (vis) sum = cadd(sum, L);
+        }
+        __syncwarp();
+    }
+    if (ri >= 0) {
+        float *o = partial + 3 * ((size_t)chunk * n_recv + ri);
+        o[0] = sum.r; o[1] = sum.g; o[2] = sum.b;
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// Persistent warp-packet gather (the production kernel).
+//
+// One resident grid (SMs x resident CTAs); every warp repeatedly takes the next work
+// item - an 8 x 4 receiver tile x a chunk of VPLs - from a global counter, so no SM idles
+// while another still holds long work (the tail of a fixed grid cost about 40% of the
+// issue slots).  Per VPL the lanes first apply only the BRDFs' early-outs (the exact zero
+// tests of lambertian.cc:63-66, phong.cc:74-77, ward.cc:104-109); the surviving lanes
+// trace their shadow rays as a packet, nearer child first by majority; the full BRDF
+// values and the clamp are evaluated only for the lanes that stay visible (about 80% of
+// traced shadow rays are occluded on the scaled scene).  Each lane adds its terms in VPL
+// order; chunk partial sums are added in chunk order by reduce_chunks_kernel.
+// ---------------------------------------------------------------------------------
+
+struct PairGeo {
+    V3 q;
+    float G;
+    V3 wi;
+    Rgb power;
+};
+
+// Geometry of a pair and the exact-zero test of its term: returns false when either
+// BRDF's early-out makes the term exactly zero (G and the power finite).
+__device__ __forceinline__ bool pair_survives(const RecvRegs &r, const rzk_vpl &l, PairGeo &pg) {
+    pg.q = ld3(l.p);
+    pg.G = form_factor_abs(r.p, r.ns, pg.q, ld3(l.n));
+    pg.wi = unit(sub(pg.q, r.p));
+    pg.power = crgb(l.contrib[0], l.contrib[1], l.contrib[2]);
+    if (isfinite(pg.G) && finite3(pg.power)) {
+        if (dot(pg.wi, r.uvn.n) <= ZERO_EPSILON || dot(r.wo, r.uvn.n) <= ZERO_EPSILON) return false;
+        if (l.mat >= 0) {
+            V3 lnn = ld3(l.nn);
+            if (dot(neg(pg.wi), lnn) <= ZERO_EPSILON || dot(ld3(l.wi), lnn) <= ZERO_EPSILON) return false;
+        }
+    }
+    return true;
+}
+
+__device__ __forceinline__ Rgb pair_radiance(const DevScene &s, const RecvRegs &r, const rzk_material &rm,
+                                             const rzk_vpl &l, const PairGeo &pg, int mode, float tau) {
+    Rgb sb = brdf_eval(rm, r.uvn, r.wo, pg.wi);
+    Rgb lb;
+    if (l.mat >= 0) {
+        rzk_material lm = load_material(s.mats + l.mat);
+        Onb lu{ld3(l.u), ld3(l.v), ld3(l.nn)};
+        lb = brdf_eval(lm, lu, ld3(l.wi), neg(pg.wi));
+    } else {
+        lb = crgb(1.0f, 1.0f, 1.0f);
+    }
+    return radiance_terms(pg.power, sb, lb, pg.G, mode, tau);
+}
+
+// Packet any-hit, nearer child first by lane majority.  Returns whether this lane's
+// segment is unoccluded (lanes with act == false return false).
+__device__ __forceinline__ bool packet_visible_near(const DevScene &s, const Ray &ray, float tmax, bool act,
+                                                    int *stk) {
+    if (s.n_nodes == 0) return act;
+    const float4 lo = __ldg(s.nodes + 2), hi = __ldg(s.nodes + 3);
+    bool alive = act && box_hit(lo, hi, ray, s.tmin, tmax);
+    if (!__any_sync(kFull, alive)) return act;
+    const int a = __float_as_int(lo.w);
+    if (a < 0) {
+        if (alive) {
+            float4 ta, tb, tc;
+            load_tri(s, -1 - a, ta, tb, tc);
+            if (tri_hit<false>(ta, tb, tc, ray, s.tmin, tmax, nullptr, nullptr, nullptr)) return false;
+        }
+        return act;
+    }
+    int top = 0;
+    stk[0] = a;
+    bool overflow = false;
+    while (top >= 0) {
+        const int c = stk[top--];
+        const float4 *pn = s.nodes + 2 * (c + 1);
+        const float4 l0 = __ldg(pn), l1 = __ldg(pn + 1), r0 = __ldg(pn + 2), r1 = __ldg(pn + 3);
+        const int al = __float_as_int(l0.w), ar = __float_as_int(r0.w);
+        float tl = 0.0f, tr = 0.0f;
+        bool hl = alive && box_hit_t(l0, l1, ray, s.tmin, tmax, tl);
+        bool hr = alive && box_hit_t(r0, r1, ray, s.tmin, tmax, tr);
+        if (al < 0 && hl) {
+            float4 ta, tb, tc;
+            load_tri(s, -1 - al, ta, tb, tc);
+            if (tri_hit<false>(ta, tb, tc, ray, s.tmin, tmax, nullptr, nullptr, nullptr)) alive = false;
+        }
+        if (ar < 0 && hr && alive) {
+            float4 ta, tb, tc;
+            load_tri(s, -1 - ar, ta, tb, tc);
+            if (tri_hit<false>(ta, tb, tc, ray, s.tmin, tmax, nullptr, nullptr, nullptr)) alive = false;
+        }
+        if (!alive) act = false;
+        const bool pl = al >= 0 && __any_sync(kFull, hl && alive);
+        const bool pr = ar >= 0 && __any_sync(kFull, hr && alive);
+        if (pl && pr) {
+            // visit the child most live lanes enter first: push it last
+            unsigned left_first = __ballot_sync(kFull, alive && hl && hr && tl <= tr);
+            unsigned right_first = __ballot_sync(kFull, alive && hl && hr && tr < tl);
+            int first = __popc(left_first) >= __popc(right_first) ? al : ar;
+            int second = first == al ? ar : al;
+            if (top < STACK_CAP - 2) { stk[++top] = second; stk[++top] = first; } else overflow = true;
+        } else if (pl) {
+            if (top < STACK_CAP - 1) stk[++top] = al; else overflow = true;
+        } else if (pr) {
+            if (top < STACK_CAP - 1) stk[++top] = ar; else overflow = true;
+        }
+        if (!__any_sync(kFull, alive)) break;
+    }
+    if (overflow && s.err) atomicOr(s.err, ERR_STACK);
+    return act;
+}
+
+template <int WARPS, int TILE, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB) gather_persistent_kernel(
+    DevScene s, const rzk_receiver *recv, int n_recv, int img_w, const rzk_vpl *vpls, int n_vpl,
+    int chunk_len, int n_chunks, int n_wtiles, int *work, int mode, float tau, float *partial) {
+    __shared__ __align__(128) rzk_vpl tiles[WARPS][2][TILE];
+    __shared__ __align__(8) uint64_t bar[WARPS][2];
+    __shared__ int stacks[WARPS][STACK_CAP];
+
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint64_t *mb = bar[w];
+    rzk_vpl(*tl)[TILE] = tiles[w];
+    int *stk = stacks[w];
+    if (lane == 0) {
+        mbar_init(&mb[0], 1);
+        mbar_init(&mb[1], 1);
+        fence_barrier_init();
+    }
+    __syncwarp();
+    uint32_t uses[2] = {0u, 0u};   // completed phases of each buffer's barrier
+    const long long n_items = (long long)n_wtiles * n_chunks;
+
+    while (true) {
+        int item = 0;
+        if (lane == 0) item = atomicAdd(work, 1);
+        item = __shfl_sync(kFull, item, 0);
+        if (item >= n_items) break;
+        const int chunk = item / n_wtiles;
+        const int wt = item - chunk * n_wtiles;
+        const int ri = lane_receiver(wt, lane, n_recv, img_w);
+        const int j0 = chunk * chunk_len;
+        const int j1 = min(n_vpl, j0 + chunk_len);
+        const int n_tiles = (j1 - j0 + TILE - 1) / TILE;
+
+        RecvRegs r;
+        r.p = mk(0.0f, 0.0f, 0.0f);   // lanes without a receiver still form (unused) rays
+        bool active = false;
+        rzk_material rm;
+        if (ri >= 0) {
+            r = load_receiver(recv + ri);
+            active = r.mat >= 0;
+            if (active) rm = load_material(s.mats + r.mat);
+        }
+        // a tile of inactive lanes contributes nothing: skip the VPL stream entirely
+        if (__any_sync(kFull, active)) {
+            Rgb sum = crgb(0.0f, 0.0f, 0.0f);
+            if (lane == 0) {
+                int cnt = min(TILE, j1 - j0);
+                fence_proxy_async();
+                mbar_expect_tx(&mb[0], cnt * (uint32_t)sizeof(rzk_vpl));
+                bulk_g2s(&tl[0][0], vpls + j0, cnt * (uint32_t)sizeof(rzk_vpl), &mb[0]);
+            }
+            bool failed = false;
+            for (int k = 0; k < n_tiles; ++k) {
+                const int buf = k & 1;
+                if (lane == 0 && k + 1 < n_tiles) {
+                    int jn = j0 + (k + 1) * TILE;
+                    int cnt = min(TILE, j1 - jn);
+                    fence_proxy_async();
+                    mbar_expect_tx(&mb[buf ^ 1], cnt * (uint32_t)sizeof(rzk_vpl));
+                    bulk_g2s(&tl[buf ^ 1][0], vpls + jn, cnt * (uint32_t)sizeof(rzk_vpl), &mb[buf ^ 1]);
+                }
+                bool ok = mbar_wait_bounded(&mb[buf], uses[buf] & 1u, lane == 0 ? s.err : nullptr);
+                uses[buf]++;
+                if (__any_sync(kFull, !ok)) { failed = true; break; }
+                const rzk_vpl *tile = tl[buf];
+                const int cnt = min(TILE, j1 - (j0 + k * TILE));
+                for (int v = 0; v < cnt; ++v) {
+                    const rzk_vpl &l = tile[v];
+                    PairGeo pg;
+                    bool act = active && pair_survives(r, l, pg);
+                    if (!__any_sync(kFull, act)) continue;
+                    Ray ray = make_ray(r.p, sub(pg.q, r.p));
+                    float tmax = len(sub(pg.q, r.p)) - s.tmin;
+                    if (packet_visible_near(s, ray, tmax, act, stk)) {
+                        Rgb L = pair_radiance(s, r, rm, l, pg, mode, tau);
+                        sum = cadd(sum, L);
+                    }
+                }
+                __syncwarp();
+            }
+            if (failed) break;
+            if (ri >= 0) {
+                float *o = partial + 3 * ((size_t)chunk * n_recv + ri);
+                o[0] = sum.r; o[1] = sum.g; o[2] = sum.b;
+            }
+        } else if (ri >= 0) {
+            float *o = partial + 3 * ((size_t)chunk * n_recv + ri);
+            o[0] = 0.0f; o[1] = 0.0f; o[2] = 0.0f;
+        }
+    }
+}
+
 __global__ void reduce_chunks_kernel(const float *partial, int n_recv, int n_chunks, float scale,
                                      float *out) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -290,26 +751,48 @@ __global__ void mean_final_kernel(const double *block_sums, int nb, int n_pairs,
 }  // namespace
 
 // Tile configurations compiled in; the autotuner picks one per workload.
+//   kind 3: persistent warp-packet kernel (the production path)      variants 0-3
+//           (2 and 3 cap registers for 5 and 6 resident 4-warp CTAs per SM)
+//   kind 1: warp-packet kernel, one CTA per receiver block            variants 4-5
+//   kind 2: warp-packet kernel on the 4-wide tree                     variant 6
+//   kind 0: per-thread block-lockstep kernel (first implementation)   variant 7
 struct GatherVariant {
-    int block, tile;
+    int kind, warps_or_block, tile;
 };
-static const GatherVariant kVariants[] = {{128, 64}, {128, 32}, {64, 64}, {64, 128}};
+static const GatherVariant kVariants[] = {
+    {3, 4, 32}, {3, 2, 32}, {3, 4, 32}, {3, 4, 32}, {1, 4, 32}, {1, 2, 32}, {2, 4, 32}, {0, 128, 64}};
 
 int gather_variant_count() { return (int)(sizeof(kVariants) / sizeof(kVariants[0])); }
 
+template <int WARPS, int TILE, int MINB>
+static int persistent_grid(rzk_context *ctx, int variant) {
+    if (ctx->persistent_grid[variant] == 0) {
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gather_persistent_kernel<WARPS, TILE, MINB>,
+                                                      WARPS * 32, 0);
+        ctx->persistent_grid[variant] = std::max(1, sms * std::max(1, per_sm));
+    }
+    return ctx->persistent_grid[variant];
+}
+
 rzk_status launch_gather(rzk_context *ctx, const DevScene &s, const rzk_receiver *recv, int n_recv,
-                         const rzk_vpl *vpls, int n_vpl, int mode, float tau, float scale,
+                         int img_w, const rzk_vpl *vpls, int n_vpl, int mode, float tau, float scale,
                          float *out, int variant, int n_chunks, cudaStream_t st) {
     if (n_recv <= 0) return RZK_OK;
     if (variant < 0 || variant >= gather_variant_count()) variant = 0;
     const GatherVariant gv = kVariants[variant];
-    const int rb = (n_recv + gv.block - 1) / gv.block;
-    const int max_chunks = std::max(1, (n_vpl + gv.tile - 1) / gv.tile);
-    if (n_chunks <= 0) {
-        int sms = 148;
-        int target = 8 * sms;
-        n_chunks = std::max(1, std::min(max_chunks, (target + rb - 1) / rb));
+    if (gv.kind == 0) img_w = 0;
+    long long wtiles;
+    if (img_w > 0) {
+        long long img_h = ((long long)n_recv + img_w - 1) / img_w;
+        wtiles = (long long)((img_w + 7) / 8) * ((img_h + 3) / 4);
+    } else {
+        wtiles = ((long long)n_recv + 31) / 32;
     }
+    const int max_chunks = std::max(1, (n_vpl + 127) / 128);
+    if (n_chunks <= 0) n_chunks = std::min(32, max_chunks);   // ~1k-VPL chunks at 32k VPLs
     n_chunks = std::min(std::min(n_chunks, max_chunks), 65535);
     if (n_vpl <= 0) n_chunks = 1;
     // chunk boundaries are multiples of 128 VPLs whatever the variant's tile, so every
@@ -325,16 +808,30 @@ rzk_status launch_gather(rzk_context *ctx, const DevScene &s, const rzk_receiver
         RZK_CUDA_TRY(cudaMalloc((void **)&ctx->d_partial, need));
         ctx->partial_bytes = need;
     }
-    dim3 grid(rb, n_chunks);
-    switch (variant) {
-        case 0: gather_kernel<128, 64><<<grid, 128, 0, st>>>(s, recv, n_recv, vpls, n_vpl, chunk_len, mode, tau, ctx->d_partial); break;
-        case 1: gather_kernel<128, 32><<<grid, 128, 0, st>>>(s, recv, n_recv, vpls, n_vpl, chunk_len, mode, tau, ctx->d_partial); break;
-        case 2: gather_kernel<64, 64><<<grid, 64, 0, st>>>(s, recv, n_recv, vpls, n_vpl, chunk_len, mode, tau, ctx->d_partial); break;
-        default: gather_kernel<64, 128><<<grid, 64, 0, st>>>(s, recv, n_recv, vpls, n_vpl, chunk_len, mode, tau, ctx->d_partial); break;
+    if (!ctx->d_work) RZK_CUDA_TRY(cudaMalloc((void **)&ctx->d_work, 64));
+    float *part = ctx->d_partial;
+    if (gv.kind == 3) {
+        RZK_CUDA_TRY(cudaMemsetAsync(ctx->d_work, 0, sizeof(int), st));
+        const int wt = (int)wtiles;
+        switch (variant) {
+            case 0: gather_persistent_kernel<4, 32, 1><<<persistent_grid<4, 32, 1>(ctx, 0), 128, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part); break;
+            case 1: gather_persistent_kernel<2, 32, 1><<<persistent_grid<2, 32, 1>(ctx, 1), 64, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part); break;
+            case 2: gather_persistent_kernel<4, 32, 5><<<persistent_grid<4, 32, 5>(ctx, 2), 128, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part); break;
+            default: gather_persistent_kernel<4, 32, 6><<<persistent_grid<4, 32, 6>(ctx, 3), 128, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part); break;
+        }
+    } else {
+        int rb = gv.kind == 0 ? (n_recv + gv.warps_or_block - 1) / gv.warps_or_block
+                              : (int)((wtiles + gv.warps_or_block - 1) / gv.warps_or_block);
+        dim3 grid(rb, n_chunks);
+        switch (variant) {
+            case 4: gather_packet_kernel<4, 32, false><<<grid, 128, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, mode, tau, part); break;
+            case 5: gather_packet_kernel<2, 32, false><<<grid, 64, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, mode, tau, part); break;
+            case 6: gather_packet_kernel<4, 32, true><<<grid, 128, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, mode, tau, part); break;
+            default: gather_kernel<128, 64><<<grid, 128, 0, st>>>(s, recv, n_recv, vpls, n_vpl, chunk_len, mode, tau, part); break;
+        }
     }
     RZK_CUDA_TRY(cudaGetLastError());
-    reduce_chunks_kernel<<<(3 * n_recv + 255) / 256, 256, 0, st>>>(ctx->d_partial, n_recv, n_chunks,
-                                                                   scale, out);
+    reduce_chunks_kernel<<<(3 * n_recv + 255) / 256, 256, 0, st>>>(part, n_recv, n_chunks, scale, out);
     RZK_CUDA_TRY(cudaGetLastError());
     return RZK_OK;
 }

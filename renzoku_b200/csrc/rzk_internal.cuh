@@ -24,6 +24,9 @@ void set_last_cuda_error(cudaError_t e, const char *what, const char *file, int 
 // Device error word bits (written by kernels, read by rzk_context_check).
 enum : uint32_t { ERR_TIMEOUT = 1u, ERR_STACK = 2u, ERR_BOUNDS = 4u };
 
+// Code of an unused entry of a 4-wide traversal node.
+constexpr int kWideEmpty = 0x7fffffff;
+
 // Area light as the VPL generator samples it (area_light.cc:27-46, quad.cc:73-87).
 struct DevLight {
     float4 p0[2], p1[2], p2[2];   // the (one or two) triangles of the light's shape
@@ -39,6 +42,7 @@ struct DevScene {
     const float4 *nodes;      // 2 x float4 per slot, slot = BFS node index + 1
     const float4 *tri_isect;  // 3 x float4 per sorted triangle (see tri_hit)
     const float4 *tri_shade;  // 2 x float4 per sorted triangle: {n, surf}, {u, -}
+    const float4 *wide;       // 8 x float4 per 4-wide traversal node (see rzk_bvh.cu K6)
     const int4 *surf;         // per surface {mat, flags, light, -}
     const rzk_material *mats;
     const DevLight *lights;
@@ -63,6 +67,9 @@ struct rzk_context {
     void *d_stage = nullptr;
     size_t stage_bytes = 0;
     double *d_mean = nullptr;
+    // work counter of the persistent gather and its resident grid size per variant
+    int *d_work = nullptr;
+    int persistent_grid[16] = {0};
 };
 
 struct rzk_scene {
@@ -86,6 +93,8 @@ struct rzk_scene {
     std::vector<int> level_first, level_last;
     // packed traversal layout
     float4 *d_nodes = nullptr, *d_tri_isect = nullptr, *d_tri_shade = nullptr;
+    float4 *d_wide = nullptr;
+    int n_wide = 0, n_wide_cap = 0;
     int4 *d_surf = nullptr;
     rzk_material *d_mats = nullptr;
     rzk::DevLight *d_lights = nullptr;
@@ -95,7 +104,7 @@ struct rzk_scene {
     // scratch for the build (freed after)
     rzk::DevScene dev() const {
         rzk::DevScene s;
-        s.nodes = d_nodes; s.tri_isect = d_tri_isect; s.tri_shade = d_tri_shade;
+        s.nodes = d_nodes; s.tri_isect = d_tri_isect; s.tri_shade = d_tri_shade; s.wide = d_wide;
         s.surf = d_surf; s.mats = d_mats; s.lights = d_lights; s.light_pdf = d_light_pdf;
         s.light_cdf = d_light_cdf; s.n_tris = n_tris; s.n_nodes = n_nodes; s.n_mats = n_mats;
         s.n_lights = n_lights; s.tmin = tmin; s.err = ctx ? ctx->d_err : nullptr;

@@ -122,6 +122,21 @@ __device__ __forceinline__ bool box_hit(float4 lo, float4 hi, const Ray &r, floa
     return (tminbox <= tmaxbox) && (tmax >= tminbox && tmaxbox >= tmin);
 }
 
+// The same test also returning the entry distance tminbox (for visit ordering only).
+__device__ __forceinline__ bool box_hit_t(float4 lo, float4 hi, const Ray &r, float tmin, float tmax,
+                                          float &tnear) {
+    float x0 = lo.x * r.inv_d.x + r.org_inv_d.x;
+    float y0 = lo.y * r.inv_d.y + r.org_inv_d.y;
+    float z0 = lo.z * r.inv_d.z + r.org_inv_d.z;
+    float x1 = hi.x * r.inv_d.x + r.org_inv_d.x;
+    float y1 = hi.y * r.inv_d.y + r.org_inv_d.y;
+    float z1 = hi.z * r.inv_d.z + r.org_inv_d.z;
+    float tminbox = smax(tmin, smax(smin(x0, x1), smax(smin(y0, y1), smin(z0, z1))));
+    float tmaxbox = smin(tmax, smin(smax(x0, x1), smin(smax(y0, y1), smax(z0, z1))));
+    tnear = tminbox;
+    return (tminbox <= tmaxbox) && (tmax >= tminbox && tmaxbox >= tmin);
+}
+
 // Triangle::hit (triangle.cc:158-275) on a packed record:
 //   a = {p0.x, p0.y, p0.z, A}, b = {B, C, D, E}, c = {F, -, -, -}
 // with (A,B,C) = p0 - p1 and (D,E,F) = p0 - p2, exactly the reference's p01 / p02.

@@ -55,8 +55,8 @@ SIGNATURES = [
     ("rzk_vpl_generate", I32, [P, U32, I32, I32, P, I32, P, P]),
     ("rzk_gather", I32, [P, P, P, I32, P, I32, I32, F32, F32, P, P]),
     ("rzk_gather_variants", I32, []),
-    ("rzk_gather_cfg", I32, [P, P, P, I32, P, I32, I32, F32, F32, P, I32, I32, P]),
-    ("rzk_gather_host", I32, [P, P, P, I32, P, I32, I32, F32, F32, P, P]),
+    ("rzk_gather_cfg", I32, [P, P, P, I32, I32, P, I32, I32, F32, F32, P, I32, I32, P]),
+    ("rzk_gather_host", I32, [P, P, P, I32, I32, P, I32, I32, F32, F32, P, P]),
     ("rzk_gather_matrix", I32, [P, P, I32, P, I32, I32, F32, P, P, P]),
     ("rzk_incident_matrix", I32, [P, P, I32, P, I32, I32, F32, P, P]),
     ("rzk_mean_contribution", I32, [P, P, P, I32, P, I32, U32, I32, P, P]),
@@ -269,24 +269,27 @@ class VirtualPointLightCuda:
         self.clamp_mode = clamp_mode
         self.clamp_threshold = clamp_threshold
 
-    def gather(self, recv, n_recv, vpls, n_vpl, scale=1.0, out=None, variant=0, n_chunks=0,
-               stream=None):
+    def gather(self, recv, n_recv, vpls, n_vpl, scale=1.0, out=None, image_width=0, variant=0,
+               n_chunks=0, stream=None):
+        """Per-receiver sum of gather_point over all VPLs, times `scale`.  image_width > 0
+        declares the receivers a row-major image (8 x 4 pixel warp tiles)."""
         torch = _torch()
         if out is None:
             out = torch.empty((n_recv, 3), dtype=torch.float32, device="cuda")
-        check(self.agg.lib.rzk_gather_cfg(self.ctx.h, self.agg.h, _dptr(recv), n_recv, _dptr(vpls),
-                                          n_vpl, self.clamp_mode, self.clamp_threshold, scale,
-                                          _dptr(out), variant, n_chunks, _stream_ptr(stream)),
+        check(self.agg.lib.rzk_gather_cfg(self.ctx.h, self.agg.h, _dptr(recv), n_recv, image_width,
+                                          _dptr(vpls), n_vpl, self.clamp_mode, self.clamp_threshold,
+                                          scale, _dptr(out), variant, n_chunks, _stream_ptr(stream)),
               "rzk_gather")
         return out
 
-    def gather_host(self, recv_np: np.ndarray, vpls_np: np.ndarray, scale=1.0) -> np.ndarray:
+    def gather_host(self, recv_np: np.ndarray, vpls_np: np.ndarray, scale=1.0,
+                    image_width=0) -> np.ndarray:
         """End-to-end call on host buffers (pinned or pageable numpy arrays)."""
         out = np.zeros((recv_np.shape[0], 3), np.float32)
         check(self.agg.lib.rzk_gather_host(self.ctx.h, self.agg.h, recv_np.ctypes.data,
-                                           recv_np.shape[0], vpls_np.ctypes.data, vpls_np.shape[0],
-                                           self.clamp_mode, self.clamp_threshold, scale,
-                                           out.ctypes.data, _stream_ptr()), "rzk_gather_host")
+                                           recv_np.shape[0], image_width, vpls_np.ctypes.data,
+                                           vpls_np.shape[0], self.clamp_mode, self.clamp_threshold,
+                                           scale, out.ctypes.data, _stream_ptr()), "rzk_gather_host")
         return out
 
     def fill(self, recv, n_recv, vpls, n_vpl, with_visibility=True, stream=None):

@@ -179,8 +179,20 @@ def test_gather_300k_against_oracle(big):
     vpls = o.vpl_generate(23, 600, 4)
     dv = rzk.records_to_device(vpls)
     ev = rzk.VirtualPointLightCuda(agg, rzk.CLAMP_RADIANCE, 0.05)
-    img = ev.gather(recv_t, recv.shape[0], dv, vpls.shape[0], scale=1.0 / 600).cpu().numpy()
+    img = ev.gather(recv_t, recv.shape[0], dv, vpls.shape[0], scale=1.0 / 600,
+                    image_width=sc.camera.width).cpu().numpy()
     ref32, ref64, cnt = o.gather(recv, vpls, rzk.CLAMP_RADIANCE, 0.05, scale=1.0 / 600, f64=True)
+    # every variant and both layouts give the same image for a fixed chunk count
+    base = None
+    for variant in range(agg.lib.rzk_gather_variants()):
+        for width in (0, sc.camera.width):
+            x = ev.gather(recv_t, recv.shape[0], dv, vpls.shape[0], scale=1.0 / 600, image_width=width,
+                          variant=variant, n_chunks=3).cpu().numpy()
+            base = x if base is None else base
+            assert np.array_equal(x, base), (variant, width)
+    one = ev.gather(recv_t, recv.shape[0], dv, vpls.shape[0], scale=1.0 / 600, n_chunks=1).cpu().numpy()
+    rel1 = np.linalg.norm(one - ref32) / np.linalg.norm(ref32)
+    assert rel1 < 1e-5, rel1
     rel32 = np.linalg.norm(img - ref32) / np.linalg.norm(ref32)
     rel64 = np.linalg.norm(img - ref64) / np.linalg.norm(ref64)
     assert rel32 < 1e-3 and rel64 < 1e-3, (rel32, rel64)
@@ -228,7 +240,7 @@ def test_gather_host_matches_device(big):
     recv = rzk.records_from_device(recv_t, sg.RECEIVER_DTYPE)
     vpls = o.vpl_generate(37, 200, 3)
     ev = rzk.VirtualPointLightCuda(agg, rzk.CLAMP_RADIANCE, 0.05)
-    a = ev.gather_host(recv, vpls, scale=0.5)
+    a = ev.gather_host(recv, vpls, scale=0.5, image_width=0)
     b = ev.gather(recv_t, recv.shape[0], rzk.records_to_device(vpls), vpls.shape[0], scale=0.5).cpu().numpy()
     assert np.array_equal(a, b)
 
