@@ -277,8 +277,9 @@ __device__ __forceinline__ bool packet_visible(const DevScene &s, const Ray &ray
         }
         return act;
     }
-    // lanes whose root test failed cannot reach any triangle below it
+    // lanes whose root test failed cannot reach any triangle below it: they stay visible
     bool alive = hit_root;
+    bool occluded = false;
     int top = 0;
     stk[0] = a;
     bool overflow = false;
@@ -292,14 +293,14 @@ __device__ __forceinline__ bool packet_visible(const DevScene &s, const Ray &ray
         if (al < 0 && hl) {
             float4 ta, tb, tc;
             load_tri(s, -1 - al, ta, tb, tc);
-            if (tri_hit<false>(ta, tb, tc, ray, s.tmin, tmax, nullptr, nullptr, nullptr)) alive = false;
+            if (tri_hit<false>(ta, tb, tc, ray, s.tmin, tmax, nullptr, nullptr, nullptr)) occluded = true;
         }
-        if (ar < 0 && hr && alive) {
+        if (ar < 0 && hr && !occluded) {
             float4 ta, tb, tc;
             load_tri(s, -1 - ar, ta, tb, tc);
-            if (tri_hit<false>(ta, tb, tc, ray, s.tmin, tmax, nullptr, nullptr, nullptr)) alive = false;
+            if (tri_hit<false>(ta, tb, tc, ray, s.tmin, tmax, nullptr, nullptr, nullptr)) occluded = true;
         }
-        if (!alive) act = false;
+        alive = alive && !occluded;
         // push order as the reference: left first, so the right child is visited next
         if (al >= 0 && __any_sync(kFull, hl && alive)) {
             if (top < STACK_CAP - 1) stk[++top] = al; else overflow = true;
@@ -310,7 +311,7 @@ __device__ __forceinline__ bool packet_visible(const DevScene &s, const Ray &ray
         if (!__any_sync(kFull, alive)) break;
     }
     if (overflow && s.err) atomicOr(s.err, ERR_STACK);
-    return act;
+    return act && !occluded;
 }
 
 // Packet any-hit over the 4-wide tree: per step one broadcast 128-byte node load, four
@@ -331,6 +332,8 @@ __device__ __forceinline__ bool packet_visible_wide(const DevScene &s, const Ray
         }
         return act;
     }
+    // lanes whose root test failed cannot reach any triangle below it: they stay visible
+    bool occluded = false;
     int top = 0;
     stk[0] = 0;
     bool overflow = false;
@@ -348,13 +351,13 @@ __device__ __forceinline__ bool packet_visible_wide(const DevScene &s, const Ray
         }
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            if (code[k] < 0 && h[k] && alive) {
+            if (code[k] < 0 && h[k] && !occluded) {
                 float4 ta, tb, tc;
                 load_tri(s, -1 - code[k], ta, tb, tc);
-                if (tri_hit<false>(ta, tb, tc, ray, s.tmin, tmax, nullptr, nullptr, nullptr)) alive = false;
+                if (tri_hit<false>(ta, tb, tc, ray, s.tmin, tmax, nullptr, nullptr, nullptr)) occluded = true;
             }
         }
-        if (!alive) act = false;
+        alive = alive && !occluded;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             if (code[k] >= 0 && code[k] != kWideEmpty && __any_sync(kFull, h[k] && alive)) {
@@ -364,7 +367,7 @@ __device__ __forceinline__ bool packet_visible_wide(const DevScene &s, const Ray
         if (!__any_sync(kFull, alive)) break;
     }
     if (overflow && s.err) atomicOr(s.err, ERR_STACK);
-    return act;
+    return act && !occluded;
 }
 
 template <int WARPS, int TILE, bool WIDE>
@@ -515,6 +518,8 @@ __device__ __forceinline__ bool packet_visible_near(const DevScene &s, const Ray
         }
         return act;
     }
+    // lanes whose root test failed cannot reach any triangle below it: they stay visible
+    bool occluded = false;
     int top = 0;
     stk[0] = a;
     bool overflow = false;
@@ -529,14 +534,14 @@ __device__ __forceinline__ bool packet_visible_near(const DevScene &s, const Ray
         if (al < 0 && hl) {
             float4 ta, tb, tc;
             load_tri(s, -1 - al, ta, tb, tc);
-            if (tri_hit<false>(ta, tb, tc, ray, s.tmin, tmax, nullptr, nullptr, nullptr)) alive = false;
+            if (tri_hit<false>(ta, tb, tc, ray, s.tmin, tmax, nullptr, nullptr, nullptr)) occluded = true;
         }
-        if (ar < 0 && hr && alive) {
+        if (ar < 0 && hr && !occluded) {
             float4 ta, tb, tc;
             load_tri(s, -1 - ar, ta, tb, tc);
-            if (tri_hit<false>(ta, tb, tc, ray, s.tmin, tmax, nullptr, nullptr, nullptr)) alive = false;
+            if (tri_hit<false>(ta, tb, tc, ray, s.tmin, tmax, nullptr, nullptr, nullptr)) occluded = true;
         }
-        if (!alive) act = false;
+        alive = alive && !occluded;
         const bool pl = al >= 0 && __any_sync(kFull, hl && alive);
         const bool pr = ar >= 0 && __any_sync(kFull, hr && alive);
         if (pl && pr) {
@@ -554,7 +559,7 @@ __device__ __forceinline__ bool packet_visible_near(const DevScene &s, const Ray
         if (!__any_sync(kFull, alive)) break;
     }
     if (overflow && s.err) atomicOr(s.err, ERR_STACK);
-    return act;
+    return act && !occluded;
 }
 
 template <int WARPS, int TILE, int MINB>
@@ -752,7 +757,8 @@ __global__ void mean_final_kernel(const double *block_sums, int nb, int n_pairs,
 
 // Tile configurations compiled in; the autotuner picks one per workload.
 //   kind 3: persistent warp-packet kernel (the production path)      variants 0-3
-//           (2 and 3 cap registers for 5 and 6 resident 4-warp CTAs per SM)
+//           (0 and 3 cap registers for 5 and 6 resident 4-warp CTAs per SM; 0 is the
+//           default, fastest on the scaled scene)
 //   kind 1: warp-packet kernel, one CTA per receiver block            variants 4-5
 //   kind 2: warp-packet kernel on the 4-wide tree                     variant 6
 //   kind 0: per-thread block-lockstep kernel (first implementation)   variant 7
@@ -814,9 +820,9 @@ rzk_status launch_gather(rzk_context *ctx, const DevScene &s, const rzk_receiver
         RZK_CUDA_TRY(cudaMemsetAsync(ctx->d_work, 0, sizeof(int), st));
         const int wt = (int)wtiles;
         switch (variant) {
-            case 0: gather_persistent_kernel<4, 32, 1><<<persistent_grid<4, 32, 1>(ctx, 0), 128, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part); break;
+            case 2: gather_persistent_kernel<4, 32, 1><<<persistent_grid<4, 32, 1>(ctx, 2), 128, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part); break;
             case 1: gather_persistent_kernel<2, 32, 1><<<persistent_grid<2, 32, 1>(ctx, 1), 64, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part); break;
-            case 2: gather_persistent_kernel<4, 32, 5><<<persistent_grid<4, 32, 5>(ctx, 2), 128, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part); break;
+            case 0: gather_persistent_kernel<4, 32, 5><<<persistent_grid<4, 32, 5>(ctx, 0), 128, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part); break;
             default: gather_persistent_kernel<4, 32, 6><<<persistent_grid<4, 32, 6>(ctx, 3), 128, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part); break;
         }
     } else {
