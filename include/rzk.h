@@ -143,6 +143,29 @@ rzk_status rzk_gather_host(rzk_context *ctx, rzk_scene *scene, const rzk_receive
                            int n_recv, int image_width, const rzk_vpl *h_vpls, int n_vpl,
                            int clamp_mode, float tau, float scale, float *h_rgb, void *stream);
 
+/* Bytes of the fixed device array that rzk_gather_noalloc uses as scratch. */
+#define RZK_NOALLOC_SCRATCH_BYTES (16u << 20)
+
+/* rzk_gather without any device allocation.  No counterpart in the reference.
+ * For callers that cannot let the library call cudaMalloc - their device memory is owned
+ * by another framework's allocator or held to a fixed budget, or they run a frame loop in
+ * which an allocation (which can synchronise the device or fail) is not acceptable.  The
+ * scratch (per-VPL-chunk partial sums and a work counter) is a fixed static device array
+ * of RZK_NOALLOC_SCRATCH_BYTES (16 MiB) that every GPU loading the library holds until
+ * the process exits; the call itself allocates and frees nothing.
+ *   - Limit: n_recv * 12 bytes must fit in the array minus 256 bytes (about 1.39 million
+ *     receivers); larger requests return RZK_ERR_CAPACITY before any device work.
+ *   - The first call on a device looks up the array's device address there (once per
+ *     device, with that device current); make that first call before any stream capture.
+ *   - All calls share the one array, and it keeps the previous call's contents: calls
+ *     whose work overlaps on the GPU (other streams, other host threads) race and must
+ *     be serialised by the caller.
+ *   - Result: the same per-receiver sums as rzk_gather, formed over as many VPL chunks
+ *     as fit (at most 32), so the float summation order can differ from rzk_gather's. */
+rzk_status rzk_gather_noalloc(rzk_scene *scene, const rzk_receiver *d_recv, int n_recv,
+                              int image_width, const rzk_vpl *d_vpls, int n_vpl, int clamp_mode,
+                              float tau, float scale, float *d_rgb, void *stream);
+
 /* LightTransportMatrix::fill (light_transport_matrix.cc:16-48): every pair's radiance
  * into a column-major rows x cols MatrixC<Rgb> (matrix_c.h:20-107) d_matrix
  * [n_vpl][n_recv][3], and optionally its visibility d_vis [n_vpl][n_recv]. */

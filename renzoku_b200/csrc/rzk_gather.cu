@@ -870,4 +870,41 @@ rzk_status launch_mean(rzk_context *ctx, const DevScene &s, const rzk_receiver *
     return RZK_OK;
 }
 
+// The persistent gather (4 warps, 32-VPL tiles, 5 CTAs per SM) on caller-provided scratch:
+// `partial` holds n_chunks x n_recv x 3 floats and `work` one int that the caller has
+// zeroed on `st`.  Used by the allocation-free entry point (rzk_noalloc.cu).
+rzk_status launch_gather_scratch(const DevScene &s, const rzk_receiver *recv, int n_recv, int img_w,
+                                 const rzk_vpl *vpls, int n_vpl, int mode, float tau, float scale,
+                                 float *out, int n_chunks, float *partial, int *work, cudaStream_t st) {
+    if (n_recv <= 0) return RZK_OK;
+    long long wtiles;
+    if (img_w > 0) {
+        long long img_h = ((long long)n_recv + img_w - 1) / img_w;
+        wtiles = (long long)((img_w + 7) / 8) * ((img_h + 3) / 4);
+    } else {
+        wtiles = ((long long)n_recv + 31) / 32;
+    }
+    if (n_vpl <= 0) n_chunks = 1;
+    int chunk_len = n_vpl > 0 ? (n_vpl + n_chunks - 1) / n_chunks : 0;
+    chunk_len = (chunk_len + 127) / 128 * 128;
+    if (chunk_len > 0) n_chunks = (n_vpl + chunk_len - 1) / chunk_len;
+    static int grid_per_device[64] = {0};
+    int dev = 0;
+    RZK_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return RZK_ERR_UNSUPPORTED;
+    if (grid_per_device[dev] == 0) {
+        int sms = 0, per_sm = 0;
+        RZK_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        RZK_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gather_persistent_kernel<4, 32, 5>,
+                                                                   128, 0));
+        grid_per_device[dev] = std::max(1, sms * std::max(1, per_sm));
+    }
+    gather_persistent_kernel<4, 32, 5><<<grid_per_device[dev], 128, 0, st>>>(
+        s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, (int)wtiles, work, mode, tau, partial);
+    RZK_CUDA_TRY(cudaGetLastError());
+    reduce_chunks_kernel<<<(3 * n_recv + 255) / 256, 256, 0, st>>>(partial, n_recv, n_chunks, scale, out);
+    RZK_CUDA_TRY(cudaGetLastError());
+    return RZK_OK;
+}
+
 }  // namespace rzk

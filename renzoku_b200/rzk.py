@@ -60,6 +60,7 @@ SIGNATURES = [
     ("rzk_gather_matrix", I32, [P, P, I32, P, I32, I32, F32, P, P, P]),
     ("rzk_incident_matrix", I32, [P, P, I32, P, I32, I32, F32, P, P]),
     ("rzk_mean_contribution", I32, [P, P, P, I32, P, I32, U32, I32, P, P]),
+    ("rzk_gather_noalloc", I32, [P, P, I32, I32, P, I32, I32, F32, F32, P, P]),
 ]
 
 _LIB = None
