@@ -507,7 +507,8 @@ __device__ __forceinline__ bool packet_visible_near(const DevScene &s, const Ray
                                                     int *stk) {
     if (s.n_nodes == 0) return act;
     const float4 lo = __ldg(s.nodes + 2), hi = __ldg(s.nodes + 3);
-    bool alive = act && box_hit(lo, hi, ray, s.tmin, tmax);
+    float t_root = 0.0f;
+    bool alive = act && box_hit_fast(lo, hi, ray, s.tmin, tmax, t_root);
     if (!__any_sync(kFull, alive)) return act;
     const int a = __float_as_int(lo.w);
     if (a < 0) {
@@ -529,8 +530,8 @@ __device__ __forceinline__ bool packet_visible_near(const DevScene &s, const Ray
         const float4 l0 = __ldg(pn), l1 = __ldg(pn + 1), r0 = __ldg(pn + 2), r1 = __ldg(pn + 3);
         const int al = __float_as_int(l0.w), ar = __float_as_int(r0.w);
         float tl = 0.0f, tr = 0.0f;
-        bool hl = alive && box_hit_t(l0, l1, ray, s.tmin, tmax, tl);
-        bool hr = alive && box_hit_t(r0, r1, ray, s.tmin, tmax, tr);
+        bool hl = alive && box_hit_fast(l0, l1, ray, s.tmin, tmax, tl);
+        bool hr = alive && box_hit_fast(r0, r1, ray, s.tmin, tmax, tr);
         if (al < 0 && hl) {
             float4 ta, tb, tc;
             load_tri(s, -1 - al, ta, tb, tc);

@@ -137,6 +137,28 @@ __device__ __forceinline__ bool box_hit_t(float4 lo, float4 hi, const Ray &r, fl
     return (tminbox <= tmaxbox) && (tmax >= tminbox && tmaxbox >= tmin);
 }
 
+// The slab test of box_hit with single-instruction min / max and one final compare, for
+// the gather's packet traversal.  With finite box bounds, ray origin and tmin / tmax
+// (receivers and VPLs are finite; |inv_d| <= 1e6 by the ZERO_EPSILON substitution of
+// ray.h:23-27) no slab value is NaN, so fminf / fmaxf select the same value as the
+// reference's (b < a) ? b : a up to the sign of a zero, which no comparison below can
+// see; and since tminbox >= tmin and tmaxbox <= tmax by construction, the reference's
+// "tmax >= tminbox && tmaxbox >= tmin" follows from tminbox <= tmaxbox.  The answer is
+// therefore the reference's answer bit for bit.
+__device__ __forceinline__ bool box_hit_fast(float4 lo, float4 hi, const Ray &r, float tmin, float tmax,
+                                             float &tnear) {
+    float x0 = lo.x * r.inv_d.x + r.org_inv_d.x;
+    float y0 = lo.y * r.inv_d.y + r.org_inv_d.y;
+    float z0 = lo.z * r.inv_d.z + r.org_inv_d.z;
+    float x1 = hi.x * r.inv_d.x + r.org_inv_d.x;
+    float y1 = hi.y * r.inv_d.y + r.org_inv_d.y;
+    float z1 = hi.z * r.inv_d.z + r.org_inv_d.z;
+    float tminbox = fmaxf(fmaxf(tmin, fminf(x0, x1)), fmaxf(fminf(y0, y1), fminf(z0, z1)));
+    float tmaxbox = fminf(fminf(tmax, fmaxf(x0, x1)), fminf(fmaxf(y0, y1), fmaxf(z0, z1)));
+    tnear = tminbox;
+    return tminbox <= tmaxbox;
+}
+
 // Triangle::hit (triangle.cc:158-275) on a packed record:
 //   a = {p0.x, p0.y, p0.z, A}, b = {B, C, D, E}, c = {F, -, -, -}
 // with (A,B,C) = p0 - p1 and (D,E,F) = p0 - p2, exactly the reference's p01 / p02.
