@@ -189,6 +189,28 @@ rzk_status rzk_mean_contribution(rzk_context *ctx, rzk_scene *scene,
                                  const rzk_vpl *d_vpls, int n_vpl, uint32_t seed,
                                  int n_pairs, double *h_mean, void *stream);
 
+/* Clustering ------------------------------------------------------------------------- */
+
+/* LightTransportMatrix::generate_alphas_for_clustering (light_transport_matrix.cc:72-106)
+ * on the column-major matrix d_matrix [cols][rows][3] (MatrixC<Rgb>, as rzk_gather_matrix
+ * writes it): d_alphas[cols]; optional d_col_norms[cols] = get_column_norms
+ * (light_transport_matrix.cc:118-130).  Bit-identical to the reference (every sum in the
+ * reference's order).  Synchronises `stream`. */
+rzk_status rzk_ltm_alphas(const float *d_matrix, int rows, int cols, float *d_alphas,
+                          float *d_col_norms, void *stream);
+
+/* ClusterBuilder::cluster_by_sampling (cluster_builder.cc:82-273) on d_matrix: centre
+ * sampling by alpha and the representatives are drawn on the host from the counter-based
+ * stream (seed, 1, 0) in the reference's order; the column-to-cluster distances and the
+ * nearest-cluster assignment run on the device.  Outputs (host): *h_n_clusters, and per
+ * final cluster its centre column, representative column and weight (capacity
+ * max(num_clusters, cols)); h_assign[cols] = final cluster of each column or -1.
+ * Synchronises `stream`. */
+rzk_status rzk_cluster_by_sampling(const float *d_matrix, int rows, int cols, int num_clusters,
+                                   uint32_t seed, int *h_n_clusters, int32_t *h_center,
+                                   int32_t *h_representative, float *h_weight,
+                                   int32_t *h_assign, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

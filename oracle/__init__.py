@@ -84,6 +84,9 @@ class Oracle:
             L.ro_draw_u32.argtypes = [U32, U32, U32, U32]
             L.ro_vpl_generate.restype = I32
             L.ro_vpl_generate.argtypes = [P, U32, I32, I32, P, I32]
+            L.ro_ltm_alphas.argtypes = [P, I32, I32, P, P]
+            L.ro_cluster_by_sampling.restype = I32
+            L.ro_cluster_by_sampling.argtypes = [P, I32, I32, I32, U32, P, P, P, P]
             cls._lib = L
         return cls._lib
 
@@ -197,6 +200,27 @@ class Oracle:
     def draw_u32(seed, stream, path, d):
         return int(Oracle.lib().ro_draw_u32(seed, stream, path, d))
 
+    @staticmethod
+    def ltm_alphas(mat):
+        """mat: float32 [cols, rows, 3] (column-major MatrixC<Rgb>)."""
+        mat = np.ascontiguousarray(mat, np.float32)
+        cols, rows = mat.shape[0], mat.shape[1]
+        a = np.zeros(cols, np.float32)
+        n = np.zeros(cols, np.float32)
+        Oracle.lib().ro_ltm_alphas(_ptr(mat), rows, cols, _ptr(a), _ptr(n))
+        return a, n
+
+    @staticmethod
+    def cluster_by_sampling(mat, num_clusters, seed):
+        mat = np.ascontiguousarray(mat, np.float32)
+        cols, rows = mat.shape[0], mat.shape[1]
+        cap = max(num_clusters, cols)
+        c = np.zeros(cap, np.int32); r = np.zeros(cap, np.int32); w = np.zeros(cap, np.float32)
+        a = np.zeros(cols, np.int32)
+        n = Oracle.lib().ro_cluster_by_sampling(_ptr(mat), rows, cols, num_clusters, seed, _ptr(c),
+                                                _ptr(r), _ptr(w), _ptr(a))
+        return c[:n], r[:n], w[:n], a
+
 
 class RefHarness:
     """The reference's own classes for one scene (see ref/ref_harness.cc)."""
@@ -232,6 +256,9 @@ class RefHarness:
             L.rref_brdf_eval.argtypes = [P, P, P, P, P, I32, P]
             L.rref_rng_stream.argtypes = [U32, U32, U32]
             L.rref_gather_mt.argtypes = [P, P, I32, P, I32, I32, F32, F32, P, I32]
+            L.rref_ltm_alphas.argtypes = [P, I32, I32, P, P]
+            L.rref_cluster_by_sampling.restype = I32
+            L.rref_cluster_by_sampling.argtypes = [P, P, I32, I32, I32, U32, P, P, P, P]
             cls._lib = L
         return cls._lib
 
@@ -307,6 +334,24 @@ class RefHarness:
         self.lib().rref_gather_mt(self.h, _ptr(recv), recv.shape[0], _ptr(vpls), vpls.shape[0],
                                   clamp_mode, tau, scale, _ptr(out), threads)
         return out
+
+    def ltm_alphas(self, mat):
+        mat = np.ascontiguousarray(mat, np.float32)
+        cols, rows = mat.shape[0], mat.shape[1]
+        a = np.zeros(cols, np.float32)
+        n = np.zeros(cols, np.float32)
+        self.lib().rref_ltm_alphas(_ptr(mat), rows, cols, _ptr(a), _ptr(n))
+        return a, n
+
+    def cluster_by_sampling(self, mat, num_clusters, seed):
+        mat = np.ascontiguousarray(mat, np.float32)
+        cols, rows = mat.shape[0], mat.shape[1]
+        cap = max(num_clusters, cols)
+        c = np.zeros(cap, np.int32); r = np.zeros(cap, np.int32); w = np.zeros(cap, np.float32)
+        a = np.zeros(cols, np.int32)
+        n = self.lib().rref_cluster_by_sampling(self.h, _ptr(mat), rows, cols, num_clusters, seed,
+                                                _ptr(c), _ptr(r), _ptr(w), _ptr(a))
+        return c[:n], r[:n], w[:n], a
 
     def incident(self, recv, vpls, clamp_mode, tau):
         n, m = recv.shape[0], vpls.shape[0]

@@ -50,6 +50,9 @@
 #include "local_geometry.h"
 #include "hitrecord.h"
 #include "log.h"
+#include "light_transport_matrix.h"
+#include "cluster_builder.h"
+#include "image_sampler.h"
 
 #include "../../include/rzk_types.h"
 #include "../../include/rzk_scene.h"
@@ -483,6 +486,54 @@ void rref_gather_mt(void *h, const rzk_receiver *recv, int n_recv, const rzk_vpl
     for (int t = 1; t < n_threads; ++t) th.emplace_back(work, t);
     work(0);
     for (auto &x : th) x.join();
+}
+
+/* LightTransportMatrix::generate_alphas_for_clustering (light_transport_matrix.cc:72-106)
+ * and get_column_norms (light_transport_matrix.cc:118-130) on a column-major matrix
+ * [cols][rows][3] (MatrixC<Rgb> layout). */
+static LightTransportMatrix *make_ltm(const float *mat, int rows, int cols) {
+    LightTransportMatrix *R = new LightTransportMatrix(rows, cols);
+    std::vector<Float> col(3 * (size_t)rows);
+    for (int j = 0; j < cols; ++j) {
+        for (int k = 0; k < 3 * rows; ++k) col[k] = mat[(size_t)j * rows * 3 + k];
+        R->set_column(j, col);
+    }
+    return R;
+}
+
+void rref_ltm_alphas(const float *mat, int rows, int cols, float *alphas, float *norms) {
+    LightTransportMatrix *R = make_ltm(mat, rows, cols);
+    std::vector<Float> a;
+    R->generate_alphas_for_clustering(a);
+    for (int j = 0; j < cols; ++j) alphas[j] = a[j];
+    std::vector<Float> n;
+    R->get_column_norms(n);
+    for (int j = 0; j < cols; ++j) norms[j] = n[j];
+    delete R;
+}
+
+/* ClusterBuilder::cluster_by_sampling (cluster_builder.cc:82-273) with its random draws from
+ * stream (seed, 1, 0).  Outputs the final clusters in order and, per column, the index of
+ * the final cluster holding it (-1 if none).  Returns the number of clusters. */
+int rref_cluster_by_sampling(void *h, const float *mat, int rows, int cols, int num_clusters, uint32_t seed,
+                             int32_t *center, int32_t *rep, float *weight, int32_t *assign) {
+    RefScene *s = (RefScene *)h;
+    LightTransportMatrix *R = make_ltm(mat, rows, cols);
+    BrdfPointLights vpls(cols);
+    Pixels pixels(rows);
+    Clusters cl;
+    ClusterBuilder cb;
+    rref_rng_stream(seed, 1u, 0u);
+    cb.cluster_by_sampling(s->scene, nullptr, *R, num_clusters, cl, vpls, pixels);
+    for (int j = 0; j < cols; ++j) assign[j] = -1;
+    for (size_t c = 0; c < cl.size(); ++c) {
+        center[c] = cl[c].center;
+        rep[c] = cl[c].representative;
+        weight[c] = cl[c].weight;
+        for (int idx : cl[c].indices) assign[idx] = (int32_t)c;
+    }
+    delete R;
+    return (int)cl.size();
 }
 
 /* incident_radiance for every (receiver, VPL) pair, column-major like rref_gather. */

@@ -1272,3 +1272,171 @@ int ro_vpl_generate(const ro_scene *s, uint32_t seed, int n_particles, int max_b
     }
     return n;
 }
+
+/* ------------------------------------------------------------------------------ */
+/* Light-transport-matrix statistics and column clustering.                        */
+/* Matrix layout: column-major [cols][rows][3] (MatrixC<Rgb>, matrix_c.h:177-184).  */
+/* ------------------------------------------------------------------------------ */
+
+/* LightTransportMatrix::generate_alphas_for_clustering (light_transport_matrix.cc:72-106)
+   and get_column_norms (light_transport_matrix.cc:118-130). */
+void ro_ltm_alphas(const float *mat, int rows, int cols, float *alphas, float *norms) {
+    float *R = (float *)malloc(sizeof(float) * (size_t)rows * cols + 4);
+    for (int j = 0; j < cols; ++j)
+        for (int i = 0; i < rows; ++i) {      /* MatrixC<Rgb>::flatten_magnitude (matrix_c.cc:49-58) */
+            const float *c = mat + 3 * ((size_t)j * rows + i);
+            R[(size_t)j * rows + i] = sqrtf(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+        }
+    float *cn = (float *)malloc(sizeof(float) * (cols + 1));
+    for (int j = 0; j < cols; ++j) {
+        float sum = 0.0f;
+        for (int i = 0; i < rows; ++i) sum += R[(size_t)j * rows + i] * R[(size_t)j * rows + i];
+        cn[j] = sqrtf(sum);
+    }
+    float *u = (float *)calloc(rows + 1, sizeof(float));   /* R.row_sum (matrix_c.h:236-245) */
+    for (int j = 0; j < cols; ++j)
+        for (int i = 0; i < rows; ++i) u[i] += R[(size_t)j * rows + i];
+    float c0 = 0.0f;                                      /* column_norms.row_sum */
+    for (int j = 0; j < cols; ++j) c0 += cn[j];
+    for (int j = 0; j < cols; ++j) {                      /* v = Rt * u (matrix_c.h:224-233) */
+        float v = 0.0f;
+        for (int i = 0; i < rows; ++i) v += R[(size_t)j * rows + i] * u[i];
+        alphas[j] = cn[j] * c0 - v;
+    }
+    if (norms) {
+        for (int j = 0; j < cols; ++j) {
+            float m = 0.0f;
+            for (int i = 0; i < rows; ++i) {
+                const float *c = mat + 3 * ((size_t)j * rows + i);
+                m += c[0] * c[0] + c[1] * c[1] + c[2] * c[2];
+            }
+            norms[j] = sqrtf(m);
+        }
+    }
+    free(R); free(cn); free(u);
+}
+
+/* DiscretePdf (pdf.cc:18-77): pdf / cdf from an array, sample by linear scan. */
+typedef struct { int n, zero; float *pdf, *cdf; } dpdf;
+static void dpdf_set(dpdf *d, const float *a, int n) {
+    d->n = n; d->zero = 0;
+    d->pdf = (float *)malloc(sizeof(float) * (n > 0 ? n : 1));
+    d->cdf = (float *)malloc(sizeof(float) * (n > 0 ? n : 1));
+    if (n == 0) { d->zero = 1; return; }
+    float sum = 0.0f;
+    for (int i = 0; i < n; ++i) sum += a[i];
+    if (sum == 0.0f) {
+        for (int i = 0; i < n; ++i) d->pdf[i] = d->cdf[i] = 0.0f;
+        d->zero = 1;
+        return;
+    }
+    for (int i = 0; i < n; ++i) d->pdf[i] = a[i] / sum;
+    d->cdf[0] = d->pdf[0];
+    for (int i = 1; i < n; ++i) d->cdf[i] = d->cdf[i - 1] + d->pdf[i];
+    d->cdf[n - 1] = 1.0f;
+}
+static void dpdf_sample(const dpdf *d, float v, int *k, float *pk) {
+    for (int i = 0; i < d->n; ++i)
+        if (v < d->cdf[i]) { *k = i; *pk = d->pdf[i]; return; }
+    *k = -1; *pk = 0.0f;
+}
+static void dpdf_free(dpdf *d) { free(d->pdf); free(d->cdf); }
+
+/* ClusterBuilder::cluster_by_sampling (cluster_builder.cc:82-273), draws from stream
+   (seed, 1, 0).  Returns the number of final clusters; assign[col] = final cluster or -1. */
+int ro_cluster_by_sampling(const float *mat, int rows, int cols, int num_clusters, uint32_t seed,
+                           int32_t *center, int32_t *rep, float *weight, int32_t *assign) {
+    for (int j = 0; j < cols; ++j) assign[j] = -1;
+    if (cols < num_clusters) {
+        for (int i = 0; i < cols; ++i) { center[i] = i; weight[i] = 1.0f; rep[i] = -1; }
+        return cols;
+    }
+    rng_t g = {seed, 1u, 0u, 0u};
+    float *alphas = (float *)malloc(sizeof(float) * (cols + 1));
+    ro_ltm_alphas(mat, rows, cols, alphas, NULL);
+    dpdf pa;
+    dpdf_set(&pa, alphas, cols);
+    int *cen = (int *)malloc(sizeof(int) * num_clusters);
+    float *w = (float *)malloc(sizeof(float) * num_clusters);
+    int count = 0;
+    while (count < num_clusters) {
+        int k; float pk;
+        dpdf_sample(&pa, rnd(&g), &k, &pk);
+        if (pk == 0.0f) continue;
+        int idx = -1;
+        for (int i = 0; i < count; ++i) if (cen[i] == k) { idx = i; break; }
+        if (idx < 0) { cen[count] = k; w[count] = 1.0f / pk; count++; }
+        else w[idx] += 1.0f / pk;
+    }
+    size_t n3 = 3 * (size_t)rows;
+    float *K = (float *)malloc(sizeof(float) * n3 * count + 4);
+    float *kn = (float *)malloc(sizeof(float) * count);
+    for (int c = 0; c < count; ++c) {
+        const float *src = mat + (size_t)cen[c] * n3;
+        for (size_t e = 0; e < n3; ++e) K[c * n3 + e] = src[e] * w[c];
+        float m = 0.0f;      /* get_column_norms */
+        for (int i = 0; i < rows; ++i) {
+            const float *v = K + c * n3 + 3 * i;
+            m += v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+        }
+        kn[c] = sqrtf(m);
+    }
+    float *mags = (float *)malloc(sizeof(float) * (cols + 1));
+    int *owner = (int *)malloc(sizeof(int) * (cols + 1));
+    int *cnt = (int *)calloc(count, sizeof(int));
+    for (int i = 0; i < cols; ++i) {
+        const float *mi = mat + (size_t)i * n3;
+        float s2 = 0.0f;                 /* magnitude(mi) (cluster_builder.cc:14-19) */
+        for (size_t e = 0; e < n3; ++e) s2 += mi[e] * mi[e];
+        float norm_mi = sqrtf(s2);
+        int min_c = -1; float min_d = 3.402823466e+38f;
+        for (int j = 0; j < count; ++j) {
+            const float *mk = K + j * n3;
+            float d = 0.0f;
+            for (size_t e = 0; e < n3; ++e) d += mi[e] * mk[e];
+            float dist = fabsf(kn[j] * norm_mi - d);
+            if (dist < min_d) { min_c = j; min_d = dist; }
+        }
+        owner[i] = min_c;
+        mags[i] = norm_mi;
+        if (min_c >= 0) cnt[min_c]++;
+    }
+    /* per-cluster member lists in column order, pdf over magnitudes, representative */
+    int n_final = 0;
+    int *map = (int *)malloc(sizeof(int) * count);
+    int **members = (int **)malloc(sizeof(int *) * count);
+    for (int c = 0; c < count; ++c) { members[c] = (int *)malloc(sizeof(int) * (cnt[c] + 1)); cnt[c] = 0; }
+    for (int i = 0; i < cols; ++i) if (owner[i] >= 0) members[owner[i]][cnt[owner[i]]++] = i;
+    int *r = (int *)malloc(sizeof(int) * count);
+    float *wf = (float *)malloc(sizeof(float) * count);
+    for (int c = 0; c < count; ++c) {
+        float *mm = (float *)malloc(sizeof(float) * (cnt[c] + 1));
+        for (int t = 0; t < cnt[c]; ++t) mm[t] = mags[members[c][t]];
+        dpdf pc;
+        dpdf_set(&pc, mm, cnt[c]);
+        int j; float pj;
+        dpdf_sample(&pc, rnd(&g), &j, &pj);
+        if (j < 0) {
+            r[c] = cnt[c] > 0 ? members[c][cnt[c] / 2] : -1;
+            wf[c] = 0.0f;
+        } else {
+            r[c] = members[c][j];
+            wf[c] = 1.0f / pj;
+        }
+        dpdf_free(&pc);
+        free(mm);
+    }
+    for (int c = 0; c < count; ++c) {
+        map[c] = -1;
+        if (r[c] >= 0) {
+            map[c] = n_final;
+            center[n_final] = cen[c]; rep[n_final] = r[c]; weight[n_final] = wf[c];
+            n_final++;
+        }
+    }
+    for (int i = 0; i < cols; ++i) assign[i] = owner[i] >= 0 ? map[owner[i]] : -1;
+    for (int c = 0; c < count; ++c) free(members[c]);
+    free(members); free(map); free(r); free(wf); free(cnt); free(owner); free(mags);
+    free(K); free(kn); free(cen); free(w); free(alphas); dpdf_free(&pa);
+    return n_final;
+}

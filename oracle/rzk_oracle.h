@@ -101,6 +101,14 @@ uint32_t ro_draw_u32(uint32_t seed, uint32_t stream, uint32_t path, uint32_t d);
 int ro_vpl_generate(const ro_scene *s, uint32_t seed, int n_particles, int max_bounce,
                     rzk_vpl *out, int cap);
 
+/* LightTransportMatrix::generate_alphas_for_clustering / get_column_norms on a
+ * column-major [cols][rows][3] matrix (light_transport_matrix.cc:72-130). */
+void ro_ltm_alphas(const float *mat, int rows, int cols, float *alphas, float *norms);
+/* ClusterBuilder::cluster_by_sampling (cluster_builder.cc:82-273), draws from stream
+ * (seed, 1, 0); returns the number of final clusters. */
+int ro_cluster_by_sampling(const float *mat, int rows, int cols, int num_clusters, uint32_t seed,
+                           int32_t *center, int32_t *rep, float *weight, int32_t *assign);
+
 #ifdef __cplusplus
 }
 #endif

@@ -61,6 +61,8 @@ SIGNATURES = [
     ("rzk_incident_matrix", I32, [P, P, I32, P, I32, I32, F32, P, P]),
     ("rzk_mean_contribution", I32, [P, P, P, I32, P, I32, U32, I32, P, P]),
     ("rzk_gather_noalloc", I32, [P, P, I32, I32, P, I32, I32, F32, F32, P, P]),
+    ("rzk_ltm_alphas", I32, [P, I32, I32, P, P, P]),
+    ("rzk_cluster_by_sampling", I32, [P, I32, I32, I32, U32, P, P, P, P, P, P]),
 ]
 
 _LIB = None
@@ -326,3 +328,35 @@ def pair_indices(seed: int, n_pairs: int, n_recv: int, n_vpl: int, draw_u32):
     ri = np.array([draw_u32(seed, 3, k, 0) % n_recv for k in range(n_pairs)], np.int32)
     vi = np.array([draw_u32(seed, 3, k, 1) % n_vpl for k in range(n_pairs)], np.int32)
     return ri, vi
+
+
+class ClusterBuilderCuda:
+    """ClusterBuilder::cluster_by_sampling (cluster_builder.h:10-27) and the matrix
+    statistics it uses, on a device matrix [cols, rows, 3] (column-major MatrixC<Rgb>)."""
+
+    def __init__(self):
+        self.lib = load()
+
+    def alphas(self, mat, stream=None):
+        torch = _torch()
+        cols, rows = mat.shape[0], mat.shape[1]
+        a = torch.empty(cols, dtype=torch.float32, device=mat.device)
+        n = torch.empty(cols, dtype=torch.float32, device=mat.device)
+        check(self.lib.rzk_ltm_alphas(_dptr(mat), rows, cols, _dptr(a), _dptr(n), _stream_ptr(stream)),
+              "rzk_ltm_alphas")
+        return a, n
+
+    def cluster_by_sampling(self, mat, num_clusters, seed, stream=None):
+        """Returns (centers, representatives, weights, assignment) as numpy arrays."""
+        cols, rows = mat.shape[0], mat.shape[1]
+        cap = max(num_clusters, cols)
+        c = np.zeros(cap, np.int32)
+        r = np.zeros(cap, np.int32)
+        w = np.zeros(cap, np.float32)
+        a = np.zeros(max(cols, 1), np.int32)
+        n = I32()
+        check(self.lib.rzk_cluster_by_sampling(_dptr(mat), rows, cols, num_clusters, seed, ctypes.byref(n),
+                                               c.ctypes.data, r.ctypes.data, w.ctypes.data, a.ctypes.data,
+                                               _stream_ptr(stream)), "rzk_cluster_by_sampling")
+        k = n.value
+        return c[:k], r[:k], w[:k], a[:cols]

@@ -67,5 +67,19 @@ def main():
         print(name, ref.n_tris, ref.n_nodes, len(vpls), {k: float(v.sum()) for k, v in images.items()})
 
 
+def clustering():
+    sys.path.insert(0, os.path.dirname(HERE))
+    from cluster_inputs import small_matrix
+    sc = sg.room_objects(120, 24, 24, seed_geo=31, seed_mat=32)
+    ref = RefHarness(sc)
+    mat = small_matrix()
+    alphas, norms = ref.ltm_alphas(mat)
+    c, r, w, a = ref.cluster_by_sampling(mat, 60, 77)
+    np.savez_compressed(os.path.join(HERE, "clustering_small.npz"), matrix_sha=digest(mat), alphas=alphas,
+                        norms=norms, center=c, rep=r, weight=w, assign=a, num_clusters=60, seed=77)
+    print("clustering", len(c))
+
+
 if __name__ == "__main__":
     main()
+    clustering()
