@@ -189,6 +189,46 @@ rzk_status rzk_mean_contribution(rzk_context *ctx, rzk_scene *scene,
                                  const rzk_vpl *d_vpls, int n_vpl, uint32_t seed,
                                  int n_pairs, double *h_mean, void *stream);
 
+/* Batched gather ----------------------------------------------------------------------- */
+
+/* One gather of a batch: the arguments of rzk_gather_cfg for one scene / image / VPL set. */
+typedef struct {
+    rzk_scene *scene;
+    const rzk_receiver *d_recv;
+    int32_t n_recv;
+    int32_t image_width;        /* as in rzk_gather_cfg; 0 = 32 consecutive receivers/warp */
+    const rzk_vpl *d_vpls;
+    int32_t n_vpl;
+    int32_t clamp_mode;
+    float tau;
+    float scale;
+    float *d_rgb;               /* n_recv x 3 output */
+} rzk_gather_job;
+
+typedef struct rzk_batch rzk_batch;
+
+/* Number of compiled batch tile configurations (warps per CTA, VPLs per tile, CTAs/SM). */
+int rzk_batch_variants(void);
+
+/* Describes a batch of independent gathers (the integrator's per-frame gather of
+ * vpl.cc:496-520 for many scenes or requests at once): uploads a device job table and
+ * allocates one partial-sum buffer.  chunk_len = VPLs per work item (a multiple of 128;
+ * 0 = rzk_gather's default).  Synchronous.  No reference counterpart (the reference
+ * renders one scene per process, integrator_scheduler.cc:54-229). */
+rzk_status rzk_batch_create(rzk_context *ctx, const rzk_gather_job *jobs, int n_jobs, int variant,
+                            int chunk_len, rzk_batch **out);
+/* Runs every job of the batch in one persistent launch: three stream operations, no
+ * allocation and no synchronisation, so it can be captured in a CUDA graph and replayed.
+ * Each job's image equals rzk_gather_cfg's for the same chunk length, bit for bit. */
+rzk_status rzk_batch_run(rzk_batch *batch, void *stream);
+rzk_status rzk_batch_destroy(rzk_batch *batch);
+/* Autotuner: times every batch variant x chunk length in {512, 1024, 2048} on up to
+ * max_probe_jobs evenly spaced jobs (0 = all) and returns the fastest.  Synchronises
+ * `stream`. */
+rzk_status rzk_batch_autotune(rzk_context *ctx, const rzk_gather_job *jobs, int n_jobs,
+                              int max_probe_jobs, int *best_variant, int *best_chunk_len,
+                              float *best_ms, void *stream);
+
 /* Clustering ------------------------------------------------------------------------- */
 
 /* LightTransportMatrix::generate_alphas_for_clustering (light_transport_matrix.cc:72-106)

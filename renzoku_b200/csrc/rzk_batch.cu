@@ -1,0 +1,278 @@
+// rzk_batch.cu - many independent gathers (different scenes, images, VPL sets, clamps) in
+// one persistent launch, and the autotuner that picks its tile configuration.
+//
+// The batch is described once (rzk_batch_create): a device table of jobs, each with its
+// scene, receivers, VPLs, clamp and output, and one partial-sum buffer for all of them.
+// rzk_batch_run then issues exactly three stream operations - zero the work counter, the
+// persistent kernel, the chunk reduction - with no allocation and no host synchronisation,
+// so it can be captured in a CUDA graph and replayed.  Work items are (job, 8 x 4 receiver
+// tile, VPL chunk), numbered job-major; every warp takes the next item from one atomic
+// counter, so small and large jobs share the SMs without a per-launch tail.  Each job's
+// image is bit-identical to rzk_gather_cfg with the same chunk length.
+#include "rzk_gather_dev.cuh"
+
+#include <algorithm>
+#include <chrono>
+#include <vector>
+
+namespace rzk {
+
+struct BatchJob {
+    DevScene s;
+    const rzk_receiver *recv;
+    const rzk_vpl *vpls;
+    float *partial;
+    float *out;
+    long long item_begin;   // first work item of this job
+    long long out_begin;    // first output float (3 per receiver) of this job in the batch
+    int n_recv, img_w, n_vpl, chunk_len, n_chunks, n_wtiles, mode;
+    float tau, scale;
+};
+
+namespace {
+
+__device__ __forceinline__ int find_job(const BatchJob *jobs, int n_jobs, long long item, bool by_out) {
+    int lo = 0, hi = n_jobs - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        long long b = by_out ? jobs[mid].out_begin : jobs[mid].item_begin;
+        if (b <= item) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <int WARPS, int TILE, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB) batch_gather_kernel(const BatchJob *jobs, int n_jobs,
+                                                                        long long n_items, int *work) {
+    __shared__ __align__(128) rzk_vpl tiles[WARPS][2][TILE];
+    __shared__ __align__(8) uint64_t bar[WARPS][2];
+    __shared__ int stacks[WARPS][STACK_CAP];
+    // each warp keeps its current job descriptor in shared memory: the fields are read
+    // where they are used instead of being held in registers across the item
+    __shared__ __align__(16) BatchJob cur[WARPS];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    WarpStage<TILE> ws;
+    ws.init(tiles[w], bar[w], stacks[w], lane);
+    int have = -1;
+    while (true) {
+        int item = 0;
+        if (lane == 0) item = atomicAdd(work, 1);
+        item = __shfl_sync(kFull, item, 0);
+        if (item >= n_items) break;
+        const int j = find_job(jobs, n_jobs, item, false);
+        if (j != have) {
+            static_assert(sizeof(BatchJob) % 4 == 0, "job copy by words");
+            const uint32_t *src = reinterpret_cast<const uint32_t *>(jobs + j);
+            uint32_t *dst = reinterpret_cast<uint32_t *>(&cur[w]);
+            for (int q = lane; q < (int)(sizeof(BatchJob) / 4); q += 32) dst[q] = src[q];
+            __syncwarp();
+            have = j;
+        }
+        const BatchJob &jb = cur[w];
+        const int local = item - (int)jb.item_begin;
+        const int chunk = local / jb.n_wtiles;
+        const int wt = local - chunk * jb.n_wtiles;
+        if (!gather_item<TILE>(jb.s, jb.recv, jb.n_recv, jb.img_w, jb.vpls, jb.n_vpl, chunk, wt, jb.chunk_len,
+                               jb.mode, jb.tau, jb.partial, ws, lane))
+            break;
+    }
+}
+
+__global__ void batch_reduce_kernel(const BatchJob *jobs, int n_jobs, long long n_out) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_out) return;
+    const int j = find_job(jobs, n_jobs, i, true);
+    const BatchJob &jb = jobs[j];
+    const long long k = i - jb.out_begin;
+    const long long stride = 3LL * jb.n_recv;
+    float acc = jb.partial[k];
+    for (int c = 1; c < jb.n_chunks; ++c) acc += jb.partial[(size_t)c * stride + k];
+    jb.out[k] = acc * jb.scale;
+}
+
+struct BatchVariant {
+    int warps, tile, minb;
+};
+const BatchVariant kBatchVariants[] = {{4, 32, 5}, {4, 32, 6}, {2, 32, 1}, {4, 16, 5}};
+
+template <int WARPS, int TILE, int MINB>
+int batch_grid() {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_gather_kernel<WARPS, TILE, MINB>, WARPS * 32, 0);
+    return std::max(1, sms * std::max(1, per_sm));
+}
+
+}  // namespace
+
+}  // namespace rzk
+
+struct rzk_batch {
+    rzk_context *ctx = nullptr;
+    rzk::BatchJob *d_jobs = nullptr;
+    float *d_partial = nullptr;
+    int *d_work = nullptr;
+    int n_jobs = 0, variant = 0, grid = 0;
+    long long n_items = 0, n_out = 0;
+    size_t partial_floats = 0;
+};
+
+using namespace rzk;
+
+extern "C" {
+
+int rzk_batch_variants(void) { return (int)(sizeof(kBatchVariants) / sizeof(kBatchVariants[0])); }
+
+rzk_status rzk_batch_destroy(rzk_batch *b) {
+    if (!b) return RZK_ERR_INVALID;
+    if (b->d_jobs) cudaFree(b->d_jobs);
+    if (b->d_partial) cudaFree(b->d_partial);
+    if (b->d_work) cudaFree(b->d_work);
+    delete b;
+    return RZK_OK;
+}
+
+rzk_status rzk_batch_create(rzk_context *ctx, const rzk_gather_job *jobs, int n_jobs, int variant, int chunk_len,
+                            rzk_batch **out) {
+    if (!ctx || !jobs || n_jobs <= 0 || !out || variant < 0 || variant >= rzk_batch_variants()) return RZK_ERR_INVALID;
+    if (chunk_len < 0 || (chunk_len % 128) != 0) return RZK_ERR_INVALID;
+    *out = nullptr;
+    std::vector<BatchJob> h(n_jobs);
+    long long items = 0, outs = 0;
+    size_t partial = 0;
+    for (int i = 0; i < n_jobs; ++i) {
+        const rzk_gather_job &g = jobs[i];
+        if (!g.scene || g.n_recv <= 0 || g.n_vpl < 0 || g.image_width < 0 || !g.d_recv || !g.d_rgb ||
+            (g.n_vpl > 0 && !g.d_vpls) || ((uintptr_t)g.d_recv & 15u) || ((uintptr_t)g.d_vpls & 15u) ||
+            g.clamp_mode < RZK_CLAMP_NONE || g.clamp_mode > RZK_CLAMP_RADIANCE)
+            return RZK_ERR_INVALID;
+        BatchJob &b = h[i];
+        b.s = g.scene->dev();
+        b.recv = g.d_recv;
+        b.vpls = g.d_vpls;
+        b.out = g.d_rgb;
+        b.n_recv = g.n_recv;
+        b.img_w = g.image_width;
+        b.n_vpl = g.n_vpl;
+        b.mode = g.clamp_mode;
+        b.tau = g.tau;
+        b.scale = g.scale;
+        long long wtiles;
+        if (b.img_w > 0) {
+            long long img_h = ((long long)b.n_recv + b.img_w - 1) / b.img_w;
+            wtiles = (long long)((b.img_w + 7) / 8) * ((img_h + 3) / 4);
+        } else {
+            wtiles = ((long long)b.n_recv + 31) / 32;
+        }
+        b.n_wtiles = (int)wtiles;
+        int cl = chunk_len;
+        if (cl == 0) {   // the default of rzk_gather: at most 32 chunks of a multiple of 128 VPLs
+            int nc = std::max(1, std::min(32, (b.n_vpl + 127) / 128));
+            cl = b.n_vpl > 0 ? (b.n_vpl + nc - 1) / nc : 0;
+            cl = (cl + 127) / 128 * 128;
+        }
+        b.chunk_len = cl;
+        b.n_chunks = (b.n_vpl > 0 && cl > 0) ? (b.n_vpl + cl - 1) / cl : 1;
+        if (b.n_vpl <= 0) b.chunk_len = 0;
+        b.item_begin = items;
+        b.out_begin = outs;
+        items += (long long)b.n_wtiles * b.n_chunks;
+        outs += 3LL * b.n_recv;
+        partial += 3ull * b.n_recv * b.n_chunks;
+    }
+    if (items >= (1LL << 30)) return RZK_ERR_CAPACITY;   // work items are counted in 32 bits
+    rzk_batch *bt = new rzk_batch();
+    bt->ctx = ctx;
+    bt->n_jobs = n_jobs;
+    bt->variant = variant;
+    bt->n_items = items;
+    bt->n_out = outs;
+    bt->partial_floats = partial;
+    auto fail = [&](cudaError_t e) {
+        set_last_cuda_error(e, "batch", __FILE__, __LINE__);
+        rzk_batch_destroy(bt);
+        return e == cudaErrorMemoryAllocation ? RZK_ERR_NOMEM : RZK_ERR_CUDA;
+    };
+    cudaError_t e = cudaMalloc((void **)&bt->d_partial, sizeof(float) * std::max<size_t>(partial, 1));
+    if (e != cudaSuccess) return fail(e);
+    size_t off = 0;
+    for (int i = 0; i < n_jobs; ++i) {
+        h[i].partial = bt->d_partial + off;
+        off += 3ull * h[i].n_recv * h[i].n_chunks;
+    }
+    if ((e = cudaMalloc((void **)&bt->d_jobs, sizeof(BatchJob) * n_jobs)) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc((void **)&bt->d_work, 64)) != cudaSuccess) return fail(e);
+    if ((e = cudaMemcpy(bt->d_jobs, h.data(), sizeof(BatchJob) * n_jobs, cudaMemcpyHostToDevice)) != cudaSuccess)
+        return fail(e);
+    switch (variant) {
+        case 0: bt->grid = batch_grid<4, 32, 5>(); break;
+        case 1: bt->grid = batch_grid<4, 32, 6>(); break;
+        case 2: bt->grid = batch_grid<2, 32, 1>(); break;
+        default: bt->grid = batch_grid<4, 16, 5>(); break;
+    }
+    *out = bt;
+    return RZK_OK;
+}
+
+rzk_status rzk_batch_run(rzk_batch *b, void *stream) {
+    if (!b) return RZK_ERR_INVALID;
+    cudaStream_t st = (cudaStream_t)stream;
+    RZK_CUDA_TRY(cudaMemsetAsync(b->d_work, 0, sizeof(int), st));
+    switch (b->variant) {
+        case 0: batch_gather_kernel<4, 32, 5><<<b->grid, 128, 0, st>>>(b->d_jobs, b->n_jobs, b->n_items, b->d_work); break;
+        case 1: batch_gather_kernel<4, 32, 6><<<b->grid, 128, 0, st>>>(b->d_jobs, b->n_jobs, b->n_items, b->d_work); break;
+        case 2: batch_gather_kernel<2, 32, 1><<<b->grid, 64, 0, st>>>(b->d_jobs, b->n_jobs, b->n_items, b->d_work); break;
+        default: batch_gather_kernel<4, 16, 5><<<b->grid, 128, 0, st>>>(b->d_jobs, b->n_jobs, b->n_items, b->d_work); break;
+    }
+    RZK_CUDA_TRY(cudaGetLastError());
+    batch_reduce_kernel<<<(unsigned)((b->n_out + 255) / 256), 256, 0, st>>>(b->d_jobs, b->n_jobs, b->n_out);
+    RZK_CUDA_TRY(cudaGetLastError());
+    return RZK_OK;
+}
+
+rzk_status rzk_batch_autotune(rzk_context *ctx, const rzk_gather_job *jobs, int n_jobs, int max_probe_jobs,
+                              int *best_variant, int *best_chunk_len, float *best_ms, void *stream) {
+    if (!ctx || !jobs || n_jobs <= 0 || !best_variant || !best_chunk_len) return RZK_ERR_INVALID;
+    // probe on an evenly spaced subset of the jobs (all of them if max_probe_jobs <= 0)
+    std::vector<rzk_gather_job> probe;
+    int k = (max_probe_jobs <= 0 || max_probe_jobs >= n_jobs) ? n_jobs : max_probe_jobs;
+    for (int i = 0; i < k; ++i) probe.push_back(jobs[(long long)i * n_jobs / k]);
+    const int chunks[] = {512, 1024, 2048};
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaEvent_t a, b;
+    RZK_CUDA_TRY(cudaEventCreate(&a));
+    RZK_CUDA_TRY(cudaEventCreate(&b));
+    float best = 3.4e38f;
+    *best_variant = 0;
+    *best_chunk_len = 1024;
+    rzk_status res = RZK_OK;
+    for (int v = 0; v < rzk_batch_variants() && res == RZK_OK; ++v) {
+        for (int c : chunks) {
+            rzk_batch *bt = nullptr;
+            res = rzk_batch_create(ctx, probe.data(), (int)probe.size(), v, c, &bt);
+            if (res != RZK_OK) break;
+            res = rzk_batch_run(bt, stream);   // warm
+            float ms = 0.0f;
+            if (res == RZK_OK) {
+                cudaEventRecord(a, st);
+                res = rzk_batch_run(bt, stream);
+                cudaEventRecord(b, st);
+                cudaEventSynchronize(b);
+                cudaEventElapsedTime(&ms, a, b);
+            }
+            rzk_batch_destroy(bt);
+            if (res == RZK_OK && ms < best) {
+                best = ms;
+                *best_variant = v;
+                *best_chunk_len = c;
+            }
+        }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (best_ms) *best_ms = best;
+    return res;
+}
+
+}  // extern "C"

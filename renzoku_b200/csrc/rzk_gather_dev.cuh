@@ -1,0 +1,303 @@
+// rzk_gather_dev.cuh - device building blocks of the gather kernels (rzk_gather.cu,
+// rzk_batch.cu): bulk-copy / mbarrier helpers, receiver and material loads, the exact-zero
+// pair test, the pair's radiance, the warp-packet any-hit and one persistent work item.
+#pragma once
+
+#include "rzk_traverse.cuh"
+
+namespace rzk {
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ void fence_barrier_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Bounded wait on a bulk-copy barrier: gives up after ~2^24 polls and reports it.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, uint32_t *err) {
+    for (uint32_t it = 0; it < (1u << 24); ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    if (err) atomicOr(err, ERR_TIMEOUT);
+    return false;
+}
+
+struct RecvRegs {
+    V3 p, ng, ns, wo;
+    Onb uvn;
+    int mat;
+};
+
+__device__ __forceinline__ RecvRegs load_receiver(const rzk_receiver *r) {
+    const float4 *q = reinterpret_cast<const float4 *>(r);
+    float4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2), d = __ldg(q + 3), e = __ldg(q + 4),
+           f = __ldg(q + 5);
+    RecvRegs o;
+    o.p = mk(a.x, a.y, a.z);
+    o.ng = mk(a.w, b.x, b.y);
+    o.ns = mk(b.z, b.w, c.x);
+    o.wo = mk(c.y, c.z, c.w);
+    o.uvn.u = mk(d.x, d.y, d.z);
+    o.uvn.v = mk(d.w, e.x, e.y);
+    o.uvn.n = mk(e.z, e.w, f.x);
+    o.mat = __float_as_int(f.y);
+    return o;
+}
+
+__device__ __forceinline__ rzk_material load_material(const rzk_material *m) {
+    const float4 *q = reinterpret_cast<const float4 *>(m);
+    float4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2);
+    rzk_material o;
+    o.type = __float_as_int(a.x);
+    o.kd[0] = a.y; o.kd[1] = a.z; o.kd[2] = a.w;
+    o.ks[0] = b.x; o.ks[1] = b.y; o.ks[2] = b.z;
+    o.p0 = b.w; o.p1 = c.x;
+    o.pad[0] = o.pad[1] = o.pad[2] = 0.0f;
+    return o;
+}
+
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ bool finite3(Rgb c) {
+    return isfinite(c.r) && isfinite(c.g) && isfinite(c.b);
+}
+
+// Receiver index of a lane: an 8 x 4 tile of a row-major image of width img_w, or 32
+// consecutive receivers when img_w == 0.  -1 outside the receiver range.
+__device__ __forceinline__ int lane_receiver(int gwarp, int lane, int n_recv, int img_w) {
+    if (img_w <= 0) {
+        int ri = gwarp * 32 + lane;
+        return ri < n_recv ? ri : -1;
+    }
+    int tiles_x = (img_w + 7) >> 3;
+    int x = (gwarp % tiles_x) * 8 + (lane & 7);
+    int y = (gwarp / tiles_x) * 4 + (lane >> 3);
+    if (x >= img_w) return -1;
+    long long ri = (long long)y * img_w + x;
+    return ri < n_recv ? (int)ri : -1;
+}
+
+struct PairGeo {
+    V3 q;
+    float G;
+    V3 wi;
+    Rgb power;
+};
+
+// Geometry of a pair and the exact-zero test of its term: returns false when either
+// BRDF's early-out makes the term exactly zero (G and the power finite).
+__device__ __forceinline__ bool pair_survives(const RecvRegs &r, const rzk_vpl &l, PairGeo &pg) {
+    pg.q = ld3(l.p);
+    pg.G = form_factor_abs(r.p, r.ns, pg.q, ld3(l.n));
+    pg.wi = unit(sub(pg.q, r.p));
+    pg.power = crgb(l.contrib[0], l.contrib[1], l.contrib[2]);
+    if (isfinite(pg.G) && finite3(pg.power)) {
+        if (dot(pg.wi, r.uvn.n) <= ZERO_EPSILON || dot(r.wo, r.uvn.n) <= ZERO_EPSILON) return false;
+        if (l.mat >= 0) {
+            V3 lnn = ld3(l.nn);
+            if (dot(neg(pg.wi), lnn) <= ZERO_EPSILON || dot(ld3(l.wi), lnn) <= ZERO_EPSILON) return false;
+        }
+    }
+    return true;
+}
+
+__device__ __forceinline__ Rgb pair_radiance(const DevScene &s, const RecvRegs &r, const rzk_material &rm,
+                                             const rzk_vpl &l, const PairGeo &pg, int mode, float tau) {
+    Rgb sb = brdf_eval(rm, r.uvn, r.wo, pg.wi);
+    Rgb lb;
+    if (l.mat >= 0) {
+        rzk_material lm = load_material(s.mats + l.mat);
+        Onb lu{ld3(l.u), ld3(l.v), ld3(l.nn)};
+        lb = brdf_eval(lm, lu, ld3(l.wi), neg(pg.wi));
+    } else {
+        lb = crgb(1.0f, 1.0f, 1.0f);
+    }
+    return radiance_terms(pg.power, sb, lb, pg.G, mode, tau);
+}
+
+// Packet any-hit, nearer child first by lane majority.  Returns whether this lane's
+// segment is unoccluded (lanes with act == false return false).
+__device__ __forceinline__ bool packet_visible_near(const DevScene &s, const Ray &ray, float tmax, bool act,
+                                                    int *stk) {
+    if (s.n_nodes == 0) return act;
+    const float4 lo = __ldg(s.nodes + 2), hi = __ldg(s.nodes + 3);
+    float t_root = 0.0f;
+    bool alive = act && box_hit_fast(lo, hi, ray, s.tmin, tmax, t_root);
+    if (!__any_sync(kFull, alive)) return act;
+    const int a = __float_as_int(lo.w);
+    if (a < 0) {
+        if (alive) {
+            float4 ta, tb, tc;
+            load_tri(s, -1 - a, ta, tb, tc);
+            if (tri_hit<false>(ta, tb, tc, ray, s.tmin, tmax, nullptr, nullptr, nullptr)) return false;
+        }
+        return act;
+    }
+    // lanes whose root test failed cannot reach any triangle below it: they stay visible
+    bool occluded = false;
+    int top = 0;
+    stk[0] = a;
+    bool overflow = false;
+    while (top >= 0) {
+        const int c = stk[top--];
+        const float4 *pn = s.nodes + 2 * (c + 1);
+        const float4 l0 = __ldg(pn), l1 = __ldg(pn + 1), r0 = __ldg(pn + 2), r1 = __ldg(pn + 3);
+        const int al = __float_as_int(l0.w), ar = __float_as_int(r0.w);
+        float tl = 0.0f, tr = 0.0f;
+        bool hl = alive && box_hit_fast(l0, l1, ray, s.tmin, tmax, tl);
+        bool hr = alive && box_hit_fast(r0, r1, ray, s.tmin, tmax, tr);
+        if (al < 0 && hl) {
+            float4 ta, tb, tc;
+            load_tri(s, -1 - al, ta, tb, tc);
+            if (tri_hit<false>(ta, tb, tc, ray, s.tmin, tmax, nullptr, nullptr, nullptr)) occluded = true;
+        }
+        if (ar < 0 && hr && !occluded) {
+            float4 ta, tb, tc;
+            load_tri(s, -1 - ar, ta, tb, tc);
+            if (tri_hit<false>(ta, tb, tc, ray, s.tmin, tmax, nullptr, nullptr, nullptr)) occluded = true;
+        }
+        alive = alive && !occluded;
+        const bool pl = al >= 0 && __any_sync(kFull, hl && alive);
+        const bool pr = ar >= 0 && __any_sync(kFull, hr && alive);
+        if (pl && pr) {
+            // visit the child most live lanes enter first: push it last
+            unsigned left_first = __ballot_sync(kFull, alive && hl && hr && tl <= tr);
+            unsigned right_first = __ballot_sync(kFull, alive && hl && hr && tr < tl);
+            int first = __popc(left_first) >= __popc(right_first) ? al : ar;
+            int second = first == al ? ar : al;
+            if (top < STACK_CAP - 2) { stk[++top] = second; stk[++top] = first; } else overflow = true;
+        } else if (pl) {
+            if (top < STACK_CAP - 1) stk[++top] = al; else overflow = true;
+        } else if (pr) {
+            if (top < STACK_CAP - 1) stk[++top] = ar; else overflow = true;
+        }
+        if (!__any_sync(kFull, alive)) break;
+    }
+    if (overflow && s.err) atomicOr(s.err, ERR_STACK);
+    return act && !occluded;
+}
+
+
+// Per-warp staging state of the persistent gathers: the warp's two VPL tiles, their
+// barriers (with the number of completed phases of each) and its packet stack.
+template <int TILE>
+struct WarpStage {
+    rzk_vpl (*tl)[TILE];
+    uint64_t *mb;
+    int *stk;
+    uint32_t uses[2];
+    __device__ __forceinline__ void init(rzk_vpl (*tiles)[TILE], uint64_t *bar, int *stack, int lane) {
+        tl = tiles;
+        mb = bar;
+        stk = stack;
+        uses[0] = uses[1] = 0u;
+        if (lane == 0) {
+            mbar_init(&mb[0], 1);
+            mbar_init(&mb[1], 1);
+            fence_barrier_init();
+        }
+        __syncwarp();
+    }
+};
+
+// One work item of the persistent gather: the 32 receivers of warp tile `wt` against VPL
+// chunk `chunk`; writes that chunk's partial sums.  Returns false if a bounded wait gave
+// up (reported in the error word).
+template <int TILE>
+__device__ __forceinline__ bool gather_item(const DevScene &s, const rzk_receiver *recv, int n_recv, int img_w,
+                                            const rzk_vpl *vpls, int n_vpl, int chunk, int wt, int chunk_len,
+                                            int mode, float tau, float *partial, WarpStage<TILE> &ws,
+                                            int lane) {
+    const int ri = lane_receiver(wt, lane, n_recv, img_w);
+    const int j0 = chunk * chunk_len;
+    const int j1 = min(n_vpl, j0 + chunk_len);
+    const int n_tiles = (j1 - j0 + TILE - 1) / TILE;
+
+    RecvRegs r;
+    r.p = mk(0.0f, 0.0f, 0.0f);   // lanes without a receiver still form (unused) rays
+    bool active = false;
+    rzk_material rm;
+    if (ri >= 0) {
+        r = load_receiver(recv + ri);
+        active = r.mat >= 0;
+        if (active) rm = load_material(s.mats + r.mat);
+    }
+    // a tile of inactive lanes contributes nothing: skip the VPL stream entirely
+    if (!__any_sync(kFull, active)) {
+        if (ri >= 0) {
+            float *o = partial + 3 * ((size_t)chunk * n_recv + ri);
+            o[0] = 0.0f; o[1] = 0.0f; o[2] = 0.0f;
+        }
+        return true;
+    }
+    Rgb sum = crgb(0.0f, 0.0f, 0.0f);
+    if (lane == 0) {
+        int cnt = min(TILE, j1 - j0);
+        fence_proxy_async();
+        mbar_expect_tx(&ws.mb[0], cnt * (uint32_t)sizeof(rzk_vpl));
+        bulk_g2s(&ws.tl[0][0], vpls + j0, cnt * (uint32_t)sizeof(rzk_vpl), &ws.mb[0]);
+    }
+    for (int k = 0; k < n_tiles; ++k) {
+        const int buf = k & 1;
+        if (lane == 0 && k + 1 < n_tiles) {
+            int jn = j0 + (k + 1) * TILE;
+            int cnt = min(TILE, j1 - jn);
+            fence_proxy_async();
+            mbar_expect_tx(&ws.mb[buf ^ 1], cnt * (uint32_t)sizeof(rzk_vpl));
+            bulk_g2s(&ws.tl[buf ^ 1][0], vpls + jn, cnt * (uint32_t)sizeof(rzk_vpl), &ws.mb[buf ^ 1]);
+        }
+        bool ok = mbar_wait_bounded(&ws.mb[buf], ws.uses[buf] & 1u, lane == 0 ? s.err : nullptr);
+        ws.uses[buf]++;
+        if (__any_sync(kFull, !ok)) return false;
+        const rzk_vpl *tile = ws.tl[buf];
+        const int cnt = min(TILE, j1 - (j0 + k * TILE));
+        for (int v = 0; v < cnt; ++v) {
+            const rzk_vpl &l = tile[v];
+            PairGeo pg;
+            bool act = active && pair_survives(r, l, pg);
+            if (!__any_sync(kFull, act)) continue;
+            Ray ray = make_ray(r.p, sub(pg.q, r.p));
+            float tmax = len(sub(pg.q, r.p)) - s.tmin;
+            if (packet_visible_near(s, ray, tmax, act, ws.stk)) {
+                Rgb L = pair_radiance(s, r, rm, l, pg, mode, tau);
+                sum = cadd(sum, L);
+            }
+        }
+        __syncwarp();
+    }
+    if (ri >= 0) {
+        float *o = partial + 3 * ((size_t)chunk * n_recv + ri);
+        o[0] = sum.r; o[1] = sum.g; o[2] = sum.b;
+    }
+    return true;
+}
+
+}  // namespace rzk

@@ -63,6 +63,11 @@ SIGNATURES = [
     ("rzk_gather_noalloc", I32, [P, P, I32, I32, P, I32, I32, F32, F32, P, P]),
     ("rzk_ltm_alphas", I32, [P, I32, I32, P, P, P]),
     ("rzk_cluster_by_sampling", I32, [P, I32, I32, I32, U32, P, P, P, P, P, P]),
+    ("rzk_batch_variants", I32, []),
+    ("rzk_batch_create", I32, [P, P, I32, I32, I32, P]),
+    ("rzk_batch_run", I32, [P, P]),
+    ("rzk_batch_destroy", I32, [P]),
+    ("rzk_batch_autotune", I32, [P, P, I32, I32, P, P, P, P]),
 ]
 
 _LIB = None
@@ -360,3 +365,55 @@ class ClusterBuilderCuda:
                                                _stream_ptr(stream)), "rzk_cluster_by_sampling")
         k = n.value
         return c[:k], r[:k], w[:k], a[:cols]
+
+
+class GatherJobC(ctypes.Structure):
+    """ctypes mirror of rzk_gather_job."""
+    _fields_ = [("scene", P), ("d_recv", P), ("n_recv", I32), ("image_width", I32), ("d_vpls", P),
+                ("n_vpl", I32), ("clamp_mode", I32), ("tau", F32), ("scale", F32), ("d_rgb", P)]
+
+
+def make_jobs(items):
+    """items: iterable of (AggregateCuda, recv tensor, n_recv, image_width, vpl tensor, n_vpl,
+    clamp_mode, tau, scale, out tensor) -> ctypes array of rzk_gather_job."""
+    items = list(items)
+    arr = (GatherJobC * len(items))()
+    for k, (agg, recv, n_recv, w, vpls, n_vpl, mode, tau, scale, out) in enumerate(items):
+        arr[k] = GatherJobC(agg.h.value, recv.data_ptr(), n_recv, w, vpls.data_ptr(), n_vpl, mode, tau,
+                            scale, out.data_ptr())
+    return arr
+
+
+class GatherBatch:
+    """Many gathers in one persistent launch (rzk_batch_*); run() is graph-capturable."""
+
+    def __init__(self, ctx: Context, jobs, variant=0, chunk_len=0):
+        self.lib = load()
+        self.jobs = jobs
+        h = ctypes.c_void_p()
+        check(self.lib.rzk_batch_create(ctx.h, jobs, len(jobs), variant, chunk_len, ctypes.byref(h)),
+              "rzk_batch_create")
+        self.h = h
+
+    def run(self, stream=None):
+        check(self.lib.rzk_batch_run(self.h, _stream_ptr(stream)), "rzk_batch_run")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.rzk_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def autotune_batch(ctx: Context, jobs, max_probe_jobs=8, stream=None):
+    """Returns (variant, chunk_len, probe_ms) of the fastest batch configuration."""
+    lib = load()
+    v, c, ms = I32(), I32(), ctypes.c_float()
+    check(lib.rzk_batch_autotune(ctx.h, jobs, len(jobs), max_probe_jobs, ctypes.byref(v), ctypes.byref(c),
+                                 ctypes.byref(ms), _stream_ptr(stream)), "rzk_batch_autotune")
+    return v.value, c.value, ms.value
