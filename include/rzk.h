@@ -217,14 +217,15 @@ int rzk_batch_variants(void);
  * renders one scene per process, integrator_scheduler.cc:54-229). */
 rzk_status rzk_batch_create(rzk_context *ctx, const rzk_gather_job *jobs, int n_jobs, int variant,
                             int chunk_len, rzk_batch **out);
-/* Runs every job of the batch in one persistent launch: three stream operations, no
- * allocation and no synchronisation, so it can be captured in a CUDA graph and replayed.
+/* Runs every job of the batch: one memset, then per table of up to 128 jobs one persistent
+ * launch and one reduction; no allocation and no synchronisation, so it can be captured in
+ * a CUDA graph and replayed.
  * Each job's image equals rzk_gather_cfg's for the same chunk length, bit for bit. */
 rzk_status rzk_batch_run(rzk_batch *batch, void *stream);
 rzk_status rzk_batch_destroy(rzk_batch *batch);
-/* Autotuner: times every batch variant x chunk length in {512, 1024, 2048} on up to
- * max_probe_jobs evenly spaced jobs (0 = all) and returns the fastest.  Synchronises
- * `stream`. */
+/* Autotuner: times every batch variant x chunk length in {default (0), 512, 1024, 2048}
+ * (best of two runs each) on up to max_probe_jobs evenly spaced jobs (0 = all) and returns
+ * the fastest.  Synchronises `stream`. */
 rzk_status rzk_batch_autotune(rzk_context *ctx, const rzk_gather_job *jobs, int n_jobs,
                               int max_probe_jobs, int *best_variant, int *best_chunk_len,
                               float *best_ms, void *stream);

@@ -1,11 +1,11 @@
 // rzk_batch.cu - many independent gathers (different scenes, images, VPL sets, clamps) in
 // one persistent launch, and the autotuner that picks its tile configuration.
 //
-// The batch is described once (rzk_batch_create): a device table of jobs, each with its
+// The batch is described once (rzk_batch_create): tables of up to 128 jobs, each with its
 // scene, receivers, VPLs, clamp and output, and one partial-sum buffer for all of them.
-// rzk_batch_run then issues exactly three stream operations - zero the work counter, the
-// persistent kernel, the chunk reduction - with no allocation and no host synchronisation,
-// so it can be captured in a CUDA graph and replayed.  Work items are (job, 8 x 4 receiver
+// rzk_batch_run then issues one memset of the work counters and, per table, the persistent
+// kernel and the chunk reduction - no allocation and no host synchronisation, so it can be
+// captured in a CUDA graph and replayed.  Work items are (job, 8 x 4 receiver
 // tile, VPL chunk), numbered job-major; every warp takes the next item from one atomic
 // counter, so small and large jobs share the SMs without a per-launch tail.  Each job's
 // image is bit-identical to rzk_gather_cfg with the same chunk length.
@@ -13,6 +13,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cstring>
 #include <vector>
 
 namespace rzk {
@@ -29,46 +30,47 @@ struct BatchJob {
     float tau, scale;
 };
 
+// Jobs travel in the launch's parameter block (a __grid_constant__ table): the kernel
+// reads each job field from the constant bank where it is used, as the single-instance
+// kernel reads its arguments, instead of holding a descriptor in registers.  Larger
+// batches are split into several launches of at most kJobsPerLaunch jobs.
+constexpr int kJobsPerLaunch = 128;
+struct JobTable {
+    BatchJob jobs[kJobsPerLaunch];
+    int n_jobs;
+    int n_items;
+    long long n_out;
+};
+static_assert(sizeof(JobTable) <= 32000, "kernel parameter block limit");
+
 namespace {
 
-__device__ __forceinline__ int find_job(const BatchJob *jobs, int n_jobs, long long item, bool by_out) {
-    int lo = 0, hi = n_jobs - 1;
+__device__ __forceinline__ int find_job(const JobTable &t, long long item, bool by_out) {
+    int lo = 0, hi = t.n_jobs - 1;
     while (lo < hi) {
         int mid = (lo + hi + 1) >> 1;
-        long long b = by_out ? jobs[mid].out_begin : jobs[mid].item_begin;
+        long long b = by_out ? t.jobs[mid].out_begin : t.jobs[mid].item_begin;
         if (b <= item) lo = mid; else hi = mid - 1;
     }
     return lo;
 }
 
 template <int WARPS, int TILE, int MINB>
-__global__ void __launch_bounds__(WARPS * 32, MINB) batch_gather_kernel(const BatchJob *jobs, int n_jobs,
-                                                                        long long n_items, int *work) {
+__global__ void __launch_bounds__(WARPS * 32, MINB) batch_gather_kernel(const __grid_constant__ JobTable t,
+                                                                        int *work) {
     __shared__ __align__(128) rzk_vpl tiles[WARPS][2][TILE];
     __shared__ __align__(8) uint64_t bar[WARPS][2];
     __shared__ int stacks[WARPS][STACK_CAP];
-    // each warp keeps its current job descriptor in shared memory: the fields are read
-    // where they are used instead of being held in registers across the item
-    __shared__ __align__(16) BatchJob cur[WARPS];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     WarpStage<TILE> ws;
     ws.init(tiles[w], bar[w], stacks[w], lane);
-    int have = -1;
     while (true) {
         int item = 0;
         if (lane == 0) item = atomicAdd(work, 1);
         item = __shfl_sync(kFull, item, 0);
-        if (item >= n_items) break;
-        const int j = find_job(jobs, n_jobs, item, false);
-        if (j != have) {
-            static_assert(sizeof(BatchJob) % 4 == 0, "job copy by words");
-            const uint32_t *src = reinterpret_cast<const uint32_t *>(jobs + j);
-            uint32_t *dst = reinterpret_cast<uint32_t *>(&cur[w]);
-            for (int q = lane; q < (int)(sizeof(BatchJob) / 4); q += 32) dst[q] = src[q];
-            __syncwarp();
-            have = j;
-        }
-        const BatchJob &jb = cur[w];
+        if (item >= t.n_items) break;
+        const int j = find_job(t, item, false);
+        const BatchJob &jb = t.jobs[j];
         const int local = item - (int)jb.item_begin;
         const int chunk = local / jb.n_wtiles;
         const int wt = local - chunk * jb.n_wtiles;
@@ -78,11 +80,11 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) batch_gather_kernel(const Ba
     }
 }
 
-__global__ void batch_reduce_kernel(const BatchJob *jobs, int n_jobs, long long n_out) {
+__global__ void batch_reduce_kernel(const __grid_constant__ JobTable t) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n_out) return;
-    const int j = find_job(jobs, n_jobs, i, true);
-    const BatchJob &jb = jobs[j];
+    if (i >= t.n_out) return;
+    const int j = find_job(t, i, true);
+    const BatchJob &jb = t.jobs[j];
     const long long k = i - jb.out_begin;
     const long long stride = 3LL * jb.n_recv;
     float acc = jb.partial[k];
@@ -93,7 +95,7 @@ __global__ void batch_reduce_kernel(const BatchJob *jobs, int n_jobs, long long 
 struct BatchVariant {
     int warps, tile, minb;
 };
-const BatchVariant kBatchVariants[] = {{4, 32, 5}, {4, 32, 6}, {2, 32, 1}, {4, 16, 5}};
+const BatchVariant kBatchVariants[] = {{4, 32, 5}, {4, 32, 4}, {2, 32, 1}, {4, 16, 5}};
 
 template <int WARPS, int TILE, int MINB>
 int batch_grid() {
@@ -110,11 +112,10 @@ int batch_grid() {
 
 struct rzk_batch {
     rzk_context *ctx = nullptr;
-    rzk::BatchJob *d_jobs = nullptr;
+    std::vector<rzk::JobTable> tables;   // one per launch; item and output offsets are per table
     float *d_partial = nullptr;
-    int *d_work = nullptr;
+    int *d_work = nullptr;               // one work counter per table
     int n_jobs = 0, variant = 0, grid = 0;
-    long long n_items = 0, n_out = 0;
     size_t partial_floats = 0;
 };
 
@@ -126,7 +127,6 @@ int rzk_batch_variants(void) { return (int)(sizeof(kBatchVariants) / sizeof(kBat
 
 rzk_status rzk_batch_destroy(rzk_batch *b) {
     if (!b) return RZK_ERR_INVALID;
-    if (b->d_jobs) cudaFree(b->d_jobs);
     if (b->d_partial) cudaFree(b->d_partial);
     if (b->d_work) cudaFree(b->d_work);
     delete b;
@@ -139,7 +139,6 @@ rzk_status rzk_batch_create(rzk_context *ctx, const rzk_gather_job *jobs, int n_
     if (chunk_len < 0 || (chunk_len % 128) != 0) return RZK_ERR_INVALID;
     *out = nullptr;
     std::vector<BatchJob> h(n_jobs);
-    long long items = 0, outs = 0;
     size_t partial = 0;
     for (int i = 0; i < n_jobs; ++i) {
         const rzk_gather_job &g = jobs[i];
@@ -175,20 +174,31 @@ rzk_status rzk_batch_create(rzk_context *ctx, const rzk_gather_job *jobs, int n_
         b.chunk_len = cl;
         b.n_chunks = (b.n_vpl > 0 && cl > 0) ? (b.n_vpl + cl - 1) / cl : 1;
         if (b.n_vpl <= 0) b.chunk_len = 0;
-        b.item_begin = items;
-        b.out_begin = outs;
-        items += (long long)b.n_wtiles * b.n_chunks;
-        outs += 3LL * b.n_recv;
+        if ((long long)b.n_wtiles * b.n_chunks >= (1LL << 30)) return RZK_ERR_CAPACITY;
         partial += 3ull * b.n_recv * b.n_chunks;
     }
-    if (items >= (1LL << 30)) return RZK_ERR_CAPACITY;   // work items are counted in 32 bits
     rzk_batch *bt = new rzk_batch();
     bt->ctx = ctx;
     bt->n_jobs = n_jobs;
     bt->variant = variant;
-    bt->n_items = items;
-    bt->n_out = outs;
     bt->partial_floats = partial;
+    // consecutive jobs go into one launch until it holds kJobsPerLaunch jobs or 2^30 items
+    for (int i = 0; i < n_jobs; ++i) {
+        long long items = (long long)h[i].n_wtiles * h[i].n_chunks;
+        if (bt->tables.empty() || bt->tables.back().n_jobs == kJobsPerLaunch ||
+            bt->tables.back().n_items + items >= (1LL << 30)) {
+            bt->tables.emplace_back();
+            JobTable &t = bt->tables.back();
+            memset(&t, 0, sizeof(t));
+        }
+        JobTable &t = bt->tables.back();
+        BatchJob &b = h[i];
+        b.item_begin = t.n_items;
+        b.out_begin = t.n_out;
+        t.n_items += (int)items;
+        t.n_out += 3LL * b.n_recv;
+        t.jobs[t.n_jobs++] = b;
+    }
     auto fail = [&](cudaError_t e) {
         set_last_cuda_error(e, "batch", __FILE__, __LINE__);
         rzk_batch_destroy(bt);
@@ -197,17 +207,15 @@ rzk_status rzk_batch_create(rzk_context *ctx, const rzk_gather_job *jobs, int n_
     cudaError_t e = cudaMalloc((void **)&bt->d_partial, sizeof(float) * std::max<size_t>(partial, 1));
     if (e != cudaSuccess) return fail(e);
     size_t off = 0;
-    for (int i = 0; i < n_jobs; ++i) {
-        h[i].partial = bt->d_partial + off;
-        off += 3ull * h[i].n_recv * h[i].n_chunks;
-    }
-    if ((e = cudaMalloc((void **)&bt->d_jobs, sizeof(BatchJob) * n_jobs)) != cudaSuccess) return fail(e);
-    if ((e = cudaMalloc((void **)&bt->d_work, 64)) != cudaSuccess) return fail(e);
-    if ((e = cudaMemcpy(bt->d_jobs, h.data(), sizeof(BatchJob) * n_jobs, cudaMemcpyHostToDevice)) != cudaSuccess)
-        return fail(e);
+    for (JobTable &t : bt->tables)
+        for (int i = 0; i < t.n_jobs; ++i) {
+            t.jobs[i].partial = bt->d_partial + off;
+            off += 3ull * t.jobs[i].n_recv * t.jobs[i].n_chunks;
+        }
+    if ((e = cudaMalloc((void **)&bt->d_work, sizeof(int) * bt->tables.size())) != cudaSuccess) return fail(e);
     switch (variant) {
         case 0: bt->grid = batch_grid<4, 32, 5>(); break;
-        case 1: bt->grid = batch_grid<4, 32, 6>(); break;
+        case 1: bt->grid = batch_grid<4, 32, 4>(); break;
         case 2: bt->grid = batch_grid<2, 32, 1>(); break;
         default: bt->grid = batch_grid<4, 16, 5>(); break;
     }
@@ -218,16 +226,20 @@ rzk_status rzk_batch_create(rzk_context *ctx, const rzk_gather_job *jobs, int n_
 rzk_status rzk_batch_run(rzk_batch *b, void *stream) {
     if (!b) return RZK_ERR_INVALID;
     cudaStream_t st = (cudaStream_t)stream;
-    RZK_CUDA_TRY(cudaMemsetAsync(b->d_work, 0, sizeof(int), st));
-    switch (b->variant) {
-        case 0: batch_gather_kernel<4, 32, 5><<<b->grid, 128, 0, st>>>(b->d_jobs, b->n_jobs, b->n_items, b->d_work); break;
-        case 1: batch_gather_kernel<4, 32, 6><<<b->grid, 128, 0, st>>>(b->d_jobs, b->n_jobs, b->n_items, b->d_work); break;
-        case 2: batch_gather_kernel<2, 32, 1><<<b->grid, 64, 0, st>>>(b->d_jobs, b->n_jobs, b->n_items, b->d_work); break;
-        default: batch_gather_kernel<4, 16, 5><<<b->grid, 128, 0, st>>>(b->d_jobs, b->n_jobs, b->n_items, b->d_work); break;
+    RZK_CUDA_TRY(cudaMemsetAsync(b->d_work, 0, sizeof(int) * b->tables.size(), st));
+    for (size_t k = 0; k < b->tables.size(); ++k) {
+        const JobTable &t = b->tables[k];
+        int *work = b->d_work + k;
+        switch (b->variant) {
+            case 0: batch_gather_kernel<4, 32, 5><<<b->grid, 128, 0, st>>>(t, work); break;
+            case 1: batch_gather_kernel<4, 32, 4><<<b->grid, 128, 0, st>>>(t, work); break;
+            case 2: batch_gather_kernel<2, 32, 1><<<b->grid, 64, 0, st>>>(t, work); break;
+            default: batch_gather_kernel<4, 16, 5><<<b->grid, 128, 0, st>>>(t, work); break;
+        }
+        RZK_CUDA_TRY(cudaGetLastError());
+        batch_reduce_kernel<<<(unsigned)((t.n_out + 255) / 256), 256, 0, st>>>(t);
+        RZK_CUDA_TRY(cudaGetLastError());
     }
-    RZK_CUDA_TRY(cudaGetLastError());
-    batch_reduce_kernel<<<(unsigned)((b->n_out + 255) / 256), 256, 0, st>>>(b->d_jobs, b->n_jobs, b->n_out);
-    RZK_CUDA_TRY(cudaGetLastError());
     return RZK_OK;
 }
 
@@ -238,14 +250,14 @@ rzk_status rzk_batch_autotune(rzk_context *ctx, const rzk_gather_job *jobs, int 
     std::vector<rzk_gather_job> probe;
     int k = (max_probe_jobs <= 0 || max_probe_jobs >= n_jobs) ? n_jobs : max_probe_jobs;
     for (int i = 0; i < k; ++i) probe.push_back(jobs[(long long)i * n_jobs / k]);
-    const int chunks[] = {512, 1024, 2048};
+    const int chunks[] = {0, 512, 1024, 2048};   // 0 = rzk_gather's per-job default
     cudaStream_t st = (cudaStream_t)stream;
     cudaEvent_t a, b;
     RZK_CUDA_TRY(cudaEventCreate(&a));
     RZK_CUDA_TRY(cudaEventCreate(&b));
     float best = 3.4e38f;
     *best_variant = 0;
-    *best_chunk_len = 1024;
+    *best_chunk_len = 0;
     rzk_status res = RZK_OK;
     for (int v = 0; v < rzk_batch_variants() && res == RZK_OK; ++v) {
         for (int c : chunks) {
@@ -253,13 +265,15 @@ rzk_status rzk_batch_autotune(rzk_context *ctx, const rzk_gather_job *jobs, int 
             res = rzk_batch_create(ctx, probe.data(), (int)probe.size(), v, c, &bt);
             if (res != RZK_OK) break;
             res = rzk_batch_run(bt, stream);   // warm
-            float ms = 0.0f;
-            if (res == RZK_OK) {
+            float ms = 3.4e38f;
+            for (int rep = 0; rep < 2 && res == RZK_OK; ++rep) {   // best of two timed runs
+                float t = 0.0f;
                 cudaEventRecord(a, st);
                 res = rzk_batch_run(bt, stream);
                 cudaEventRecord(b, st);
                 cudaEventSynchronize(b);
-                cudaEventElapsedTime(&ms, a, b);
+                cudaEventElapsedTime(&t, a, b);
+                ms = std::min(ms, t);
             }
             rzk_batch_destroy(bt);
             if (res == RZK_OK && ms < best) {
