@@ -252,6 +252,93 @@ rzk_status rzk_cluster_by_sampling(const float *d_matrix, int rows, int cols, in
                                    int32_t *h_representative, float *h_weight,
                                    int32_t *h_assign, void *stream);
 
+/* LightSlice ------------------------------------------------------------------------- */
+
+/* LightSlice's settings (lightslice.h:306-312, lightslice.cc:23-85). */
+typedef struct {
+    int32_t num_clusters;         /* global VPL clusters (num_clusters) */
+    int32_t max_slice_size;       /* kd-tree leaf capacity that makes a slice (>= 2) */
+    int32_t num_neighbor_slices;  /* rows of a slice's matrix L */
+    int32_t max_slice_clusters;   /* per-slice refinement stops at this many clusters */
+    int32_t map_resolution;       /* Jensen map side (luminance_map_resolution) */
+    float map_epsilon;            /* luminance_map_epsilon */
+    float density_radius;         /* estimate_sum's disk radius */
+    int32_t incident_clamp_mode;  /* clamp of incident_radiance in the reduced matrix */
+    float incident_tau;
+    uint32_t seed;                /* streams (seed,4,0) slicing, (seed,1,0) clustering, (seed,5,s) refinement */
+    int32_t n_threads;            /* host threads refining slices (0 = all cores) */
+} rzk_lightslice_params;
+
+typedef struct rzk_lightslice rzk_lightslice;
+
+/* The reference's defaults (lightslice.cc:23-85; seed 2013 as random.h:21). */
+rzk_status rzk_lightslice_params_default(rzk_lightslice_params *params);
+
+/* LightSlice::initialize (lightslice.cc:589-1277) for one image: d_recv are the width x
+ * height primary receivers (row-major, as rzk_primary writes them), d_vpls the VPL set (only
+ * VPLs of bounce <= 1 are used, lightslice.cc:606-613).  Slices the shading points with the
+ * 6-D kd-tree (lightslice.cc:252-303), traces the reduced matrix of the slice
+ * representatives on the device, clusters its columns (cluster_builder.cc:82-273), refines
+ * the clusters per slice (lightslice.cc:789-1060), and builds the per-slice Jensen maps
+ * (lightslice.cc:2058-2151).  The maps are built for the slices whose VPL sum is positive:
+ * the reference calls build_map before it sets the sampling records' is_valid (still
+ * value-initialised false), which would leave every map empty.  Synchronous. */
+rzk_status rzk_lightslice_create(rzk_context *ctx, rzk_scene *scene, const rzk_receiver *d_recv, int width,
+                                 int height, const rzk_vpl *d_vpls, int n_vpl,
+                                 const rzk_lightslice_params *params, rzk_lightslice **out, void *stream);
+rzk_status rzk_lightslice_destroy(rzk_lightslice *ls);
+/* Sizes and the host time of each build stage (h_ms[8]: points+filter, slicing, reduced
+ * matrix, global clustering, refinement, maps, tables). */
+rzk_status rzk_lightslice_info(const rzk_lightslice *ls, int32_t *n_points, int32_t *n_slices,
+                               int32_t *n_vpl_used, int32_t *n_global_clusters, int32_t *n_slice_clusters,
+                               double *h_ms);
+/* Slicing dump: per kd-tree data position its pixel; per slice [start, end], representative
+ * (a data position) and its nearest slices (num_neighbor_slices each, furthest first, -1
+ * padded).  Any pointer may be NULL. */
+rzk_status rzk_lightslice_slices(const rzk_lightslice *ls, int32_t *h_point_pixel, int32_t *h_start,
+                                 int32_t *h_end, int32_t *h_rep, int32_t *h_neighbors);
+/* Per-slice clusters, slice-major: h_count[n_slices]; per cluster its representative
+ * (one-bounce VPL index), weight, upper-hemisphere flag, direction to the representative,
+ * total incident radiance, probability in the slice's cluster distribution, member count;
+ * h_members the members of every cluster in order.  Any pointer may be NULL. */
+rzk_status rzk_lightslice_clusters(const rzk_lightslice *ls, int32_t *h_count, int32_t *h_rep, float *h_weight,
+                                   uint8_t *h_upper, float *h_wi, float *h_incident, float *h_pdf,
+                                   int32_t *h_size, int32_t *h_members);
+/* Jensen maps [slice][res][res] (row-major, row = y), validity, VPL sum, row CDFs
+ * [slice][res] and column CDFs [slice][res][res] (DiscretePdf2D, pdf.cc:195-229). */
+rzk_status rzk_lightslice_maps(const rzk_lightslice *ls, float *h_maps, uint8_t *h_valid, float *h_sum,
+                               float *h_row_cdf, float *h_col_cdf);
+/* The reduced matrix (column-major [n_vpl_used][n_slices][3]) and visibility, copied to
+ * device buffers, and the input index of every one-bounce VPL.  Any pointer may be NULL. */
+rzk_status rzk_lightslice_matrix(const rzk_lightslice *ls, float *d_R, uint8_t *d_V, int32_t *h_vpl_index,
+                                 void *stream);
+/* KdTreeN::find_cluster with the plane bias (kdtree_n.h:486-518) for every receiver: its
+ * slice, or -1 without a material. */
+rzk_status rzk_lightslice_find_slice(rzk_lightslice *ls, const rzk_receiver *d_recv, int n_recv,
+                                     int32_t *d_slice, void *stream);
+/* Host-input forms of the two host stages, for callers that computed the points, the
+ * reduced matrix or the global clusters elsewhere (and for checking those stages on their
+ * own).  rzk_lightslice_host_slice: the 6-D points [n][6] with their pixels, in pixel order
+ * -> slices, representatives, neighbours.  rzk_lightslice_host_refine: the reduced matrix
+ * [n_vpl_used][n_slices][3] and visibility of that slicing, the used VPLs, each slice's
+ * representative receiver, the global clusters (representative, weight), each column's
+ * cluster and magnitude -> per-slice clusters, distributions and maps.  Objects made this
+ * way have no device tables: gather and find_slice return RZK_ERR_INVALID on them. */
+rzk_status rzk_lightslice_host_slice(const rzk_lightslice_params *params, const float *h_points,
+                                     const int32_t *h_pixel, int n_points, rzk_lightslice **out);
+rzk_status rzk_lightslice_host_refine(rzk_lightslice *ls, const float *h_R, const uint8_t *h_V, int n_vpl_used,
+                                      const rzk_vpl *h_vpls_used, const rzk_receiver *h_rep_recv,
+                                      int n_global, const int32_t *h_global_rep, const float *h_global_weight,
+                                      const int32_t *h_assign, const float *h_mags);
+/* KdTreeN::find_cluster (kdtree_n.h:486-518) on the host for 6-D points [n][6]. */
+rzk_status rzk_lightslice_host_find(const rzk_lightslice *ls, const float *h_points, int n, int32_t *h_slice);
+/* LightSlice::gather_clusters (lightslice.cc:1315-1345) for every receiver, times `scale`
+ * (1 / num_emitted_photons, vpl.cc:487-490): the sum over its slice's clusters of
+ * weight x radiance(representative) where visible, in cluster order.  Receivers without a
+ * material get black. */
+rzk_status rzk_lightslice_gather(rzk_lightslice *ls, const rzk_receiver *d_recv, int n_recv, int clamp_mode,
+                                 float tau, float scale, float *d_rgb, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -478,6 +478,7 @@ rzk_status bvh_build(rzk_scene *s, cudaStream_t st) {
     int rb = std::min(1024, grid);
     box_reduce_kernel<<<rb, 256, 0, st>>>(s->d_bmin, s->d_bmax, n, box + 6);
     box_final_kernel<<<1, 32, 0, st>>>(box + 6, rb, box);
+    RZK_CUDA_TRY(cudaMemcpyAsync(s->box, box, sizeof(float) * 6, cudaMemcpyDeviceToHost, st));
     morton_kernel<<<grid, TB, 0, st>>>(s->d_bmin, s->d_bmax, n, box, s->d_codes, s->d_perm);
     RZK_CUDA_TRY(cudaGetLastError());
 

@@ -26,9 +26,6 @@ rzk_status launch_gather(rzk_context *ctx, const DevScene &s, const rzk_receiver
                          int img_w, const rzk_vpl *vpls, int n_vpl, int mode, float tau, float scale,
                          float *out, int variant, int n_chunks, cudaStream_t st);
 int gather_variant_count();
-rzk_status launch_matrix(const DevScene &s, const rzk_receiver *recv, int n_recv, const rzk_vpl *vpls,
-                         int n_vpl, int mode, float tau, float *mat, uint8_t *vis, bool incident,
-                         cudaStream_t st);
 rzk_status launch_mean(rzk_context *ctx, const DevScene &s, const rzk_receiver *recv, int n_recv,
                        const rzk_vpl *vpls, int n_vpl, uint32_t seed, int n_pairs, double *h_mean,
                        cudaStream_t st);
@@ -370,7 +367,7 @@ rzk_status rzk_gather_matrix(rzk_scene *s, const rzk_receiver *d_recv, int n_rec
                              void *stream) {
     if (!s || n_recv < 0 || n_vpl < 0 || (n_recv && n_vpl && !d_matrix)) return RZK_ERR_INVALID;
     if (clamp_mode < RZK_CLAMP_NONE || clamp_mode > RZK_CLAMP_RADIANCE) return RZK_ERR_INVALID;
-    return launch_matrix(s->dev(), d_recv, n_recv, d_vpls, n_vpl, clamp_mode, tau, d_matrix, d_vis, false,
+    return launch_matrix(s->dev(), d_recv, n_recv, d_vpls, n_vpl, clamp_mode, tau, d_matrix, d_vis, 0,
                          as_stream(stream));
 }
 
@@ -378,7 +375,7 @@ rzk_status rzk_incident_matrix(rzk_scene *s, const rzk_receiver *d_recv, int n_r
                                int n_vpl, int clamp_mode, float tau, float *d_matrix, void *stream) {
     if (!s || n_recv < 0 || n_vpl < 0 || (n_recv && n_vpl && !d_matrix)) return RZK_ERR_INVALID;
     if (clamp_mode < RZK_CLAMP_NONE || clamp_mode > RZK_CLAMP_RADIANCE) return RZK_ERR_INVALID;
-    return launch_matrix(s->dev(), d_recv, n_recv, d_vpls, n_vpl, clamp_mode, tau, d_matrix, nullptr, true,
+    return launch_matrix(s->dev(), d_recv, n_recv, d_vpls, n_vpl, clamp_mode, tau, d_matrix, nullptr, 1,
                          as_stream(stream));
 }
 

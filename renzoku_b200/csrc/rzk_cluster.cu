@@ -14,6 +14,8 @@
 // one representative per cluster) are sequential and stay on the host, drawing from the
 // counter-based stream (seed, 1, 0) in the reference's order.
 #include "rzk_internal.cuh"
+#include "rzk_hostutil.h"
+#include "rzk_cluster.cuh"
 
 #include <algorithm>
 #include <vector>
@@ -152,53 +154,6 @@ __global__ void argmin_kernel(const float *D, int cols, int count, int *owner) {
     owner[i] = best;
 }
 
-struct DPdf {   // DiscretePdf (pdf.cc:18-77)
-    std::vector<float> pdf, cdf;
-    bool monotone = true;
-    void set(const float *a, int n) {
-        pdf.assign(n, 0.0f);
-        cdf.assign(n, 0.0f);
-        if (n == 0) return;
-        float sum = 0.0f;
-        for (int i = 0; i < n; ++i) sum += a[i];
-        if (sum == 0.0f) return;
-        for (int i = 0; i < n; ++i) pdf[i] = a[i] / sum;
-        cdf[0] = pdf[0];
-        for (int i = 1; i < n; ++i) cdf[i] = cdf[i - 1] + pdf[i];
-        cdf[n - 1] = 1.0f;
-        for (int i = 1; i < n; ++i)
-            if (cdf[i] < cdf[i - 1]) { monotone = false; break; }
-    }
-    // first i with v < cdf[i] (linear scan semantics; a binary search where the cdf is
-    // non-decreasing finds the same index)
-    void sample(float v, int &k, float &pk) const {
-        int n = (int)cdf.size();
-        if (monotone) {
-            int lo = 0, hi = n;
-            while (lo < hi) {
-                int mid = (lo + hi) >> 1;
-                if (v < cdf[mid]) hi = mid; else lo = mid + 1;
-            }
-            if (lo < n) { k = lo; pk = pdf[lo]; return; }
-        } else {
-            for (int i = 0; i < n; ++i)
-                if (v < cdf[i]) { k = i; pk = pdf[i]; return; }
-        }
-        k = -1;
-        pk = 0.0f;
-    }
-};
-
-struct HostRng {   // Random::operator() on the counter-based stream (random.h:60-63)
-    uint32_t seed, stream, path, d = 0;
-    float next() {
-        uint4 blk = philox4x32_10(make_uint4(d >> 2, path, stream, 0x52454e5au), seed, 0x4b5a4f52u);
-        uint32_t w = (d & 3) == 0 ? blk.x : ((d & 3) == 1 ? blk.y : ((d & 3) == 2 ? blk.z : blk.w));
-        d++;
-        return (w & 0x00ffffffu) * (1.0f / 16777216.0f);
-    }
-};
-
 template <class T>
 struct DevBuf {
     T *p = nullptr;
@@ -225,7 +180,7 @@ rzk_status ltm_alphas(const float *mat, int rows, int cols, float *alphas, float
 
 rzk_status cluster_by_sampling(const float *mat, int rows, int cols, int num_clusters, uint32_t seed,
                                int *h_n, int32_t *h_center, int32_t *h_rep, float *h_weight,
-                               int32_t *h_assign, cudaStream_t st) {
+                               int32_t *h_assign, cudaStream_t st, float *h_mags) {
     for (int j = 0; j < cols; ++j) h_assign[j] = -1;
     if (cols < num_clusters) {   // cluster_builder.cc:90-101
         for (int i = 0; i < cols; ++i) { h_center[i] = i; h_weight[i] = 1.0f; h_rep[i] = -1; }
@@ -285,6 +240,7 @@ rzk_status cluster_by_sampling(const float *mat, int rows, int cols, int num_clu
     RZK_CUDA_TRY(cudaMemcpyAsync(owner.data(), d_owner.p, sizeof(int) * cols, cudaMemcpyDeviceToHost, st));
     RZK_CUDA_TRY(cudaMemcpyAsync(mags.data(), nm.p, sizeof(float) * cols, cudaMemcpyDeviceToHost, st));
     RZK_CUDA_TRY(cudaStreamSynchronize(st));
+    if (h_mags) std::copy(mags.begin(), mags.end(), h_mags);
     // members in column order, pdf over magnitudes, representative (cluster_builder.cc:228-272)
     std::vector<std::vector<int>> members(count);
     for (int i = 0; i < cols; ++i)

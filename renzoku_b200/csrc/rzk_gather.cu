@@ -399,12 +399,15 @@ __global__ void reduce_chunks_kernel(const float *partial, int n_recv, int n_chu
     out[i] = acc * scale;
 }
 
-// LightTransportMatrix::fill: every pair, visibility always traced.
+// LightTransportMatrix::fill: every pair, visibility always traced.  kind 0: radiance
+// (gather_point, lights skipped); kind 1: incident radiance without visibility; kind 2:
+// (float)visible x incident radiance, the reduced matrix of LightSlice
+// (lightslice.cc:721-737), with the visibility written as well.
 constexpr int kMatBlock = 128;
 __global__ void __launch_bounds__(kMatBlock) matrix_kernel(DevScene s, const rzk_receiver *recv,
                                                            int n_recv, const rzk_vpl *vpls, int n_vpl,
                                                            int mode, float tau, float *mat,
-                                                           uint8_t *vis, int incident) {
+                                                           uint8_t *vis, int kind) {
     __shared__ int stack_mem[STACK_CAP * kMatBlock];
     const int ri = blockIdx.x * kMatBlock + threadIdx.x;
     if (ri >= n_recv) return;
@@ -415,7 +418,7 @@ __global__ void __launch_bounds__(kMatBlock) matrix_kernel(DevScene s, const rzk
     rzk_vpl l = vpls[j];
     Rgb L = crgb(0.0f, 0.0f, 0.0f);
     bool visible = false;
-    if (incident) {
+    if (kind >= 1) {
         // VirtualPointLight::incident_radiance (vpl.cc:411-440): geometric normal, no
         // visibility, surface BRDF white.
         V3 q = ld3(l.p);
@@ -429,6 +432,13 @@ __global__ void __launch_bounds__(kMatBlock) matrix_kernel(DevScene s, const rzk
         }
         L = radiance_terms(crgb(l.contrib[0], l.contrib[1], l.contrib[2]), crgb(1.0f, 1.0f, 1.0f),
                            lb, G, mode, tau);
+        if (kind == 2) {
+            Ray ray = make_ray(r.p, sub(q, r.p));
+            float tmax = len(sub(q, r.p)) - s.tmin;
+            visible = !any_hit<kMatBlock, false>(s, ray, s.tmin, tmax, stk);
+            const float vf = visible ? 1.0f : 0.0f;
+            L = crgb(vf * L.r, vf * L.g, vf * L.b);
+        }
     } else if (r.mat >= 0) {
         V3 q = ld3(l.p);
         Ray ray = make_ray(r.p, sub(q, r.p));
@@ -579,12 +589,11 @@ rzk_status launch_gather(rzk_context *ctx, const DevScene &s, const rzk_receiver
 }
 
 rzk_status launch_matrix(const DevScene &s, const rzk_receiver *recv, int n_recv, const rzk_vpl *vpls,
-                         int n_vpl, int mode, float tau, float *mat, uint8_t *vis, bool incident,
+                         int n_vpl, int mode, float tau, float *mat, uint8_t *vis, int kind,
                          cudaStream_t st) {
     if (n_recv <= 0 || n_vpl <= 0) return RZK_OK;
     dim3 grid((n_recv + kMatBlock - 1) / kMatBlock, std::min(n_vpl, 65535));
-    matrix_kernel<<<grid, kMatBlock, 0, st>>>(s, recv, n_recv, vpls, n_vpl, mode, tau, mat, vis,
-                                              incident ? 1 : 0);
+    matrix_kernel<<<grid, kMatBlock, 0, st>>>(s, recv, n_recv, vpls, n_vpl, mode, tau, mat, vis, kind);
     RZK_CUDA_TRY(cudaGetLastError());
     return RZK_OK;
 }

@@ -230,12 +230,13 @@ struct WarpStage {
 
 // One work item of the persistent gather: the 32 receivers of warp tile `wt` against VPL
 // chunk `chunk`; writes that chunk's partial sums.  Returns false if a bounded wait gave
-// up (reported in the error word).
-template <int TILE>
+// up (reported in the error word).  WEIGHTED: VPL j's radiance is multiplied by
+// weights[j] before it is added (a cluster representative standing for its cluster).
+template <int TILE, bool WEIGHTED = false>
 __device__ __forceinline__ bool gather_item(const DevScene &s, const rzk_receiver *recv, int n_recv, int img_w,
                                             const rzk_vpl *vpls, int n_vpl, int chunk, int wt, int chunk_len,
                                             int mode, float tau, float *partial, WarpStage<TILE> &ws,
-                                            int lane) {
+                                            int lane, const float *weights = nullptr) {
     const int ri = lane_receiver(wt, lane, n_recv, img_w);
     const int j0 = chunk * chunk_len;
     const int j1 = min(n_vpl, j0 + chunk_len);
@@ -250,8 +251,9 @@ __device__ __forceinline__ bool gather_item(const DevScene &s, const rzk_receive
         active = r.mat >= 0;
         if (active) rm = load_material(s.mats + r.mat);
     }
-    // a tile of inactive lanes contributes nothing: skip the VPL stream entirely
-    if (!__any_sync(kFull, active)) {
+    // a tile of inactive lanes, or an empty chunk, contributes nothing: no VPL stream (an
+    // empty chunk must not arm a barrier phase that no wait consumes)
+    if (n_tiles <= 0 || !__any_sync(kFull, active)) {
         if (ri >= 0) {
             float *o = partial + 3 * ((size_t)chunk * n_recv + ri);
             o[0] = 0.0f; o[1] = 0.0f; o[2] = 0.0f;
@@ -288,6 +290,10 @@ __device__ __forceinline__ bool gather_item(const DevScene &s, const rzk_receive
             float tmax = len(sub(pg.q, r.p)) - s.tmin;
             if (packet_visible_near(s, ray, tmax, act, ws.stk)) {
                 Rgb L = pair_radiance(s, r, rm, l, pg, mode, tau);
+                if (WEIGHTED) {
+                    const float w = weights[j0 + k * TILE + v];
+                    L = crgb(w * L.r, w * L.g, w * L.b);
+                }
                 sum = cadd(sum, L);
             }
         }

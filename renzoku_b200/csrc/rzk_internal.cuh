@@ -76,6 +76,7 @@ struct rzk_scene {
     rzk_context *ctx = nullptr;
     int n_tris = 0, n_nodes = 0, n_levels = 0, n_surfs = 0, n_mats = 0, n_lights = 0;
     float tmin = 1e-3f;
+    float box[6] = {0, 0, 0, 0, 0, 0};   // Aggregate::box (min xyz, max xyz), incl. the origin
     // original (flattened, input-order) triangles
     float *d_v = nullptr;        // [n][9]
     float *d_tp = nullptr;       // [n][3] tangent reference vertex
@@ -119,4 +120,9 @@ rzk_status bvh_build(rzk_scene *s, cudaStream_t st);
 rzk_status exclusive_scan_i32(const int *d_in, int *d_out, int n, int *d_total, void *d_tmp,
                               size_t tmp_bytes, cudaStream_t st);
 size_t exclusive_scan_tmp_bytes(int n);
+// rzk_gather.cu: every (receiver, VPL) pair into a column-major [n_vpl][n_recv][3] matrix;
+// kind 0 radiance, 1 incident radiance, 2 visible x incident radiance (+ visibility)
+rzk_status launch_matrix(const DevScene &s, const rzk_receiver *recv, int n_recv, const rzk_vpl *vpls,
+                         int n_vpl, int mode, float tau, float *mat, uint8_t *vis, int kind,
+                         cudaStream_t st);
 }  // namespace rzk

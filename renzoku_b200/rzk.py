@@ -68,6 +68,19 @@ SIGNATURES = [
     ("rzk_batch_run", I32, [P, P]),
     ("rzk_batch_destroy", I32, [P]),
     ("rzk_batch_autotune", I32, [P, P, I32, I32, P, P, P, P]),
+    ("rzk_lightslice_params_default", I32, [P]),
+    ("rzk_lightslice_create", I32, [P, P, P, I32, I32, P, I32, P, P, P]),
+    ("rzk_lightslice_destroy", I32, [P]),
+    ("rzk_lightslice_info", I32, [P, P, P, P, P, P, P]),
+    ("rzk_lightslice_slices", I32, [P, P, P, P, P, P]),
+    ("rzk_lightslice_clusters", I32, [P, P, P, P, P, P, P, P, P, P]),
+    ("rzk_lightslice_maps", I32, [P, P, P, P, P, P]),
+    ("rzk_lightslice_matrix", I32, [P, P, P, P, P]),
+    ("rzk_lightslice_find_slice", I32, [P, P, I32, P, P]),
+    ("rzk_lightslice_host_slice", I32, [P, P, P, I32, P]),
+    ("rzk_lightslice_host_refine", I32, [P, P, P, I32, P, P, I32, P, P, P, P]),
+    ("rzk_lightslice_host_find", I32, [P, P, I32, P]),
+    ("rzk_lightslice_gather", I32, [P, P, I32, I32, F32, F32, P, P]),
 ]
 
 _LIB = None
@@ -417,3 +430,157 @@ def autotune_batch(ctx: Context, jobs, max_probe_jobs=8, stream=None):
     check(lib.rzk_batch_autotune(ctx.h, jobs, len(jobs), max_probe_jobs, ctypes.byref(v), ctypes.byref(c),
                                  ctypes.byref(ms), _stream_ptr(stream)), "rzk_batch_autotune")
     return v.value, c.value, ms.value
+
+
+class LightSliceParamsC(ctypes.Structure):
+    """ctypes mirror of rzk_lightslice_params."""
+    _fields_ = [("num_clusters", I32), ("max_slice_size", I32), ("num_neighbor_slices", I32),
+                ("max_slice_clusters", I32), ("map_resolution", I32), ("map_epsilon", F32),
+                ("density_radius", F32), ("incident_clamp_mode", I32), ("incident_tau", F32),
+                ("seed", U32), ("n_threads", I32)]
+
+
+def lightslice_params(**kw) -> LightSliceParamsC:
+    """The reference's defaults (lightslice.cc:23-85) with keyword overrides."""
+    p = LightSliceParamsC()
+    check(load().rzk_lightslice_params_default(ctypes.byref(p)), "rzk_lightslice_params_default")
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+class LightSliceCuda:
+    """LightSlice (lightslice.cc): slicing, reduced matrix, clustering, per-slice refinement and
+    maps built from an image's receivers and a VPL set; gather() is gather_clusters for every
+    pixel.  Built from host inputs (from_host) it holds the host stages only."""
+
+    def __init__(self, handle, params, lib=None, agg=None):
+        self.lib = lib or load()
+        self.h = handle
+        self.params = params
+        self.agg = agg
+
+    @classmethod
+    def create(cls, agg: "AggregateCuda", recv, width: int, height: int, vpls, n_vpl: int, params=None,
+               stream=None):
+        params = params or lightslice_params()
+        h = ctypes.c_void_p()
+        check(agg.lib.rzk_lightslice_create(agg.ctx.h, agg.h, _dptr(recv), width, height, _dptr(vpls), n_vpl,
+                                            ctypes.byref(params), ctypes.byref(h), _stream_ptr(stream)),
+              "rzk_lightslice_create")
+        return cls(h, params, agg.lib, agg)
+
+    @classmethod
+    def from_host(cls, params, points: np.ndarray, pixels: np.ndarray):
+        lib = load()
+        pts = np.ascontiguousarray(points, np.float32)
+        pix = np.ascontiguousarray(pixels, np.int32)
+        h = ctypes.c_void_p()
+        check(lib.rzk_lightslice_host_slice(ctypes.byref(params), pts.ctypes.data, pix.ctypes.data, len(pix),
+                                            ctypes.byref(h)), "rzk_lightslice_host_slice")
+        return cls(h, params, lib)
+
+    def host_refine(self, R: np.ndarray, V: np.ndarray, vpls_used: np.ndarray, rep_recv: np.ndarray,
+                    g_rep, g_weight, assign, mags):
+        R = np.ascontiguousarray(R, np.float32)
+        V = np.ascontiguousarray(V, np.uint8)
+        vpls_used = np.ascontiguousarray(vpls_used)
+        rep_recv = np.ascontiguousarray(rep_recv)
+        g_rep = np.ascontiguousarray(g_rep, np.int32)
+        g_weight = np.ascontiguousarray(g_weight, np.float32)
+        assign = np.ascontiguousarray(assign, np.int32)
+        mags = np.ascontiguousarray(mags, np.float32)
+        check(self.lib.rzk_lightslice_host_refine(self.h, R.ctypes.data, V.ctypes.data, len(vpls_used),
+                                                  vpls_used.ctypes.data, rep_recv.ctypes.data, len(g_rep),
+                                                  g_rep.ctypes.data, g_weight.ctypes.data, assign.ctypes.data,
+                                                  mags.ctypes.data), "rzk_lightslice_host_refine")
+
+    def info(self):
+        v = [I32() for _ in range(5)]
+        ms = (ctypes.c_double * 8)()
+        check(self.lib.rzk_lightslice_info(self.h, *[ctypes.byref(x) for x in v], ms), "rzk_lightslice_info")
+        n_points, n_slices, n_vpl, n_global, n_sc = [x.value for x in v]
+        return {"points": n_points, "slices": n_slices, "vpls_used": n_vpl, "global_clusters": n_global,
+                "slice_clusters": n_sc, "ms": list(ms)}
+
+    def slices(self):
+        inf = self.info()
+        ns, k = inf["slices"], self.params.num_neighbor_slices
+        pp = np.zeros(inf["points"], np.int32)
+        st, en, rp = (np.zeros(ns, np.int32) for _ in range(3))
+        nb = np.zeros((ns, k), np.int32)
+        check(self.lib.rzk_lightslice_slices(self.h, pp.ctypes.data, st.ctypes.data, en.ctypes.data, rp.ctypes.data,
+                                             nb.ctypes.data), "rzk_lightslice_slices")
+        return {"point_pixel": pp, "start": st, "end": en, "rep": rp, "neighbors": nb}
+
+    def clusters(self):
+        inf = self.info()
+        ns, nc = inf["slices"], inf["slice_clusters"]
+        cnt = np.zeros(ns, np.int32)
+        rep, size = np.zeros(nc, np.int32), np.zeros(nc, np.int32)
+        w, pdf = np.zeros(nc, np.float32), np.zeros(nc, np.float32)
+        up = np.zeros(nc, np.uint8)
+        wi, inc = np.zeros((nc, 3), np.float32), np.zeros((nc, 3), np.float32)
+        check(self.lib.rzk_lightslice_clusters(self.h, cnt.ctypes.data, rep.ctypes.data, w.ctypes.data,
+                                               up.ctypes.data, wi.ctypes.data, inc.ctypes.data, pdf.ctypes.data,
+                                               size.ctypes.data, None), "rzk_lightslice_clusters")
+        mem = np.zeros(int(size.sum()), np.int32)
+        check(self.lib.rzk_lightslice_clusters(self.h, None, None, None, None, None, None, None, None,
+                                               mem.ctypes.data), "rzk_lightslice_clusters")
+        return {"count": cnt, "rep": rep, "weight": w, "upper": up, "wi": wi, "incident": inc, "pdf": pdf,
+                "size": size, "members": mem}
+
+    def maps(self):
+        ns, res = self.info()["slices"], self.params.map_resolution
+        m = np.zeros((ns, res, res), np.float32)
+        v = np.zeros(ns, np.uint8)
+        sm = np.zeros(ns, np.float32)
+        rc = np.zeros((ns, res), np.float32)
+        cc = np.zeros((ns, res, res), np.float32)
+        check(self.lib.rzk_lightslice_maps(self.h, m.ctypes.data, v.ctypes.data, sm.ctypes.data, rc.ctypes.data,
+                                           cc.ctypes.data), "rzk_lightslice_maps")
+        return {"maps": m, "valid": v, "sum": sm, "row_cdf": rc, "col_cdf": cc}
+
+    def matrix(self):
+        torch = _torch()
+        inf = self.info()
+        ns, n1 = inf["slices"], inf["vpls_used"]
+        R = torch.empty((n1, ns, 3), dtype=torch.float32, device="cuda")
+        V = torch.empty((n1, ns), dtype=torch.uint8, device="cuda")
+        idx = np.zeros(n1, np.int32)
+        check(self.lib.rzk_lightslice_matrix(self.h, _dptr(R), _dptr(V), idx.ctypes.data, _stream_ptr()),
+              "rzk_lightslice_matrix")
+        return R, V, idx
+
+    def host_find(self, points: np.ndarray) -> np.ndarray:
+        pts = np.ascontiguousarray(points, np.float32)
+        out = np.zeros(len(pts), np.int32)
+        check(self.lib.rzk_lightslice_host_find(self.h, pts.ctypes.data, len(pts), out.ctypes.data),
+              "rzk_lightslice_host_find")
+        return out
+
+    def find_slice(self, recv, n_recv, stream=None):
+        torch = _torch()
+        out = torch.empty(n_recv, dtype=torch.int32, device="cuda")
+        check(self.lib.rzk_lightslice_find_slice(self.h, _dptr(recv), n_recv, _dptr(out), _stream_ptr(stream)),
+              "rzk_lightslice_find_slice")
+        return out
+
+    def gather(self, recv, n_recv, clamp_mode, tau, scale=1.0, out=None, stream=None):
+        torch = _torch()
+        if out is None:
+            out = torch.empty((n_recv, 3), dtype=torch.float32, device="cuda")
+        check(self.lib.rzk_lightslice_gather(self.h, _dptr(recv), n_recv, clamp_mode, tau, scale, _dptr(out),
+                                             _stream_ptr(stream)), "rzk_lightslice_gather")
+        return out
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.rzk_lightslice_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
