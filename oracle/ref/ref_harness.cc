@@ -22,74 +22,11 @@
  * drags in the closed LibImportance headers, so their few lines are repeated here
  * calling the reference's own Aggregate, FormFactor, Material and RadianceTerms.
  */
-#include <cstdint>
-#include <cstring>
-#include <vector>
-#include <string>
-#include <thread>
+#include "ref_common.h"
 
-#include "common.h"
-#include "vec3.h"
-#include "rgb.h"
-#include "triangle.h"
-#include "quad.h"
-#include "surface.h"
-#include "material.h"
-#include "lambertian.h"
-#include "phong.h"
-#include "ward.h"
-#include "area_light.h"
-#include "aggregate_bvh.h"
-#include "camera.h"
-#include "sensor.h"
-#include "scene.h"
-#include "random.h"
-#include "form_factor.h"
-#include "vpl_interface.h"
-#include "vpl_generator.h"
-#include "local_geometry.h"
-#include "hitrecord.h"
-#include "log.h"
-#include "light_transport_matrix.h"
-#include "cluster_builder.h"
-#include "image_sampler.h"
+using namespace rref;
 
-#include "../../include/rzk_types.h"
-#include "../../include/rzk_scene.h"
-
-using namespace Renzoku;
-
-extern "C" void rref_rng_stream(uint32_t seed, uint32_t stream, uint32_t path);
-
-namespace {
-
-/* Exposes the protected build products of the reference BVH for dumping. */
-class BvhProbe : public AggregateBvh {
-public:
-    explicit BvhProbe(Surfaces &s) : AggregateBvh(s) {}
-    const BvhNode *node_array() const { return nodes; }
-    int node_count() const { return num_nodes; }
-    const unsigned int *morton() const { return sorted_morton; }
-    const int *surface_ids() const { return sorted_surface_id; }
-    const Triangle *tris() const { return sorted_triangles; }
-    int tri_count() const { return num_triangles; }
-};
-
-struct RefScene {
-    Shapes *shapes = nullptr;
-    Materials *materials = nullptr;
-    Textures *textures = nullptr;
-    Surfaces *surfaces = nullptr;
-    Lights *lights = nullptr;
-    Camera *camera = nullptr;
-    Sensor *sensor = nullptr;
-    Random *rd = nullptr;
-    BvhProbe *bvh = nullptr;
-    Scene *scene = nullptr;
-    std::vector<int> tri_first;   /* first flattened triangle of each primitive */
-    std::vector<int> tri_count;
-    float tmin = RAY_TMIN;
-};
+namespace rref {
 
 Vec3 v3(const float *f) { return Vec3(f[0], f[1], f[2]); }
 void put3(float *dst, const Vec3 &v) { dst[0] = v.x(); dst[1] = v.y(); dst[2] = v.z(); }
@@ -195,7 +132,7 @@ void fill_receiver(const Ray &r, const HitRecord &rec, rzk_receiver &out,
     out.flags = 1;
 }
 
-}  // namespace
+}  // namespace rref
 
 /* Camera request for the harness: eye, lookat, up, vertical fov in degrees,
  * image and film sizes.  The harness builds the reference Camera from it the way
