@@ -259,6 +259,24 @@ class RefHarness:
             L.rref_ltm_alphas.argtypes = [P, I32, I32, P, P]
             L.rref_cluster_by_sampling.restype = I32
             L.rref_cluster_by_sampling.argtypes = [P, P, I32, I32, I32, U32, P, P, P, P]
+            L.rref_ls_create.restype = P
+            L.rref_ls_create.argtypes = [P, I32, I32, U32]
+            L.rref_ls_num_points.restype = I32
+            L.rref_ls_num_points.argtypes = [P]
+            L.rref_ls_num_slices.restype = I32
+            L.rref_ls_num_slices.argtypes = [P]
+            L.rref_ls_points.argtypes = [P, P, P]
+            L.rref_ls_slices.argtypes = [P, P, P, P, P]
+            L.rref_ls_neighbors.argtypes = [P, P]
+            L.rref_ls_find.argtypes = [P, P, I32, P]
+            L.rref_ls_reduced_matrix.restype = I32
+            L.rref_ls_reduced_matrix.argtypes = [P, P, I32, I32, F32, P, P, P]
+            L.rref_ls_refine.argtypes = [P, P, P, I32, I32, P, P, P, P, I32, U32, I32, F32, F32]
+            L.rref_ls_num_slice_clusters.restype = I32
+            L.rref_ls_num_slice_clusters.argtypes = [P]
+            L.rref_ls_clusters.argtypes = [P, P, P, P, P, P, P, P, P, P, P]
+            L.rref_ls_maps.argtypes = [P, P, P, P, P]
+            L.rref_ls_gather.argtypes = [P, P, I32, I32, F32, P]
             cls._lib = L
         return cls._lib
 
@@ -364,3 +382,106 @@ class RefHarness:
         out = np.zeros((n, 3), np.float32)
         self.lib().rref_brdf_eval(self.h, _ptr(mat), _ptr(uvn9), _ptr(wo), _ptr(wi), n, _ptr(out))
         return out
+
+    def lightslice(self, max_slice_size: int, num_neighbors: int, seed: int):
+        """LightSlice::generate_slices on this scene (stream (seed, 4, 0))."""
+        return RefLightSlice(self, max_slice_size, num_neighbors, seed)
+
+
+class RefLightSlice:
+    """The reference's LightSlice stages on a RefHarness scene (see ref/ls_harness.cc)."""
+
+    def __init__(self, ref: RefHarness, max_slice_size: int, num_neighbors: int, seed: int):
+        self.ref = ref
+        self.k = num_neighbors
+        L = RefHarness.lib()
+        self.h = L.rref_ls_create(ref.h, max_slice_size, num_neighbors, seed)
+        self.n_points = L.rref_ls_num_points(self.h)
+        self.n_slices = L.rref_ls_num_slices(self.h)
+        self.n_vpl1 = 0
+        self.res = 0
+
+    def points(self):
+        pts = np.zeros((self.n_points, 6), np.float32)
+        pix = np.zeros(self.n_points, np.int32)
+        RefHarness.lib().rref_ls_points(self.h, _ptr(pts), _ptr(pix))
+        return pts, pix
+
+    def slices(self):
+        ns = self.n_slices
+        pp = np.zeros(self.n_points, np.int32)
+        st, en, rp = (np.zeros(ns, np.int32) for _ in range(3))
+        RefHarness.lib().rref_ls_slices(self.h, _ptr(pp), _ptr(st), _ptr(en), _ptr(rp))
+        nb = np.zeros((ns, self.k), np.int32)
+        RefHarness.lib().rref_ls_neighbors(self.h, _ptr(nb))
+        return {"point_pixel": pp, "start": st, "end": en, "rep": rp, "neighbors": nb}
+
+    def find(self, pts):
+        pts = np.ascontiguousarray(pts, np.float32)
+        out = np.zeros(len(pts), np.int32)
+        RefHarness.lib().rref_ls_find(self.h, _ptr(pts), len(pts), _ptr(out))
+        return out
+
+    def reduced_matrix(self, vpls, inc_mode=0, inc_tau=0.0):
+        vpls = np.ascontiguousarray(vpls)
+        n1 = int((vpls["bounce"] <= 1).sum())
+        R = np.zeros((n1, self.n_slices, 3), np.float32)
+        V = np.zeros((n1, self.n_slices), np.uint8)
+        rep = np.zeros(self.n_slices, sg.RECEIVER_DTYPE)
+        got = RefHarness.lib().rref_ls_reduced_matrix(self.h, _ptr(vpls), len(vpls), inc_mode, inc_tau, _ptr(R),
+                                                      _ptr(V), _ptr(rep))
+        assert got == n1
+        self.n_vpl1 = n1
+        return R, V, rep
+
+    def refine(self, R, V, g_rep, g_weight, assign, mags, max_slice_clusters, seed, res=32, eps=1e-3,
+               density_radius=0.1):
+        R = np.ascontiguousarray(R, np.float32)
+        V = np.ascontiguousarray(V, np.uint8)
+        g_rep = np.ascontiguousarray(g_rep, np.int32)
+        g_weight = np.ascontiguousarray(g_weight, np.float32)
+        assign = np.ascontiguousarray(assign, np.int32)
+        mags = np.ascontiguousarray(mags, np.float32)
+        self.res = res
+        RefHarness.lib().rref_ls_refine(self.h, _ptr(R), _ptr(V), R.shape[0], len(g_rep), _ptr(g_rep),
+                                        _ptr(g_weight), _ptr(assign), _ptr(mags), max_slice_clusters, seed, res,
+                                        eps, density_radius)
+
+    def clusters(self):
+        L = RefHarness.lib()
+        nc = L.rref_ls_num_slice_clusters(self.h)
+        cnt = np.zeros(self.n_slices, np.int32)
+        rep, size = np.zeros(nc, np.int32), np.zeros(nc, np.int32)
+        w, pdf = np.zeros(nc, np.float32), np.zeros(nc, np.float32)
+        up = np.zeros(nc, np.uint8)
+        wi, inc = np.zeros((nc, 3), np.float32), np.zeros((nc, 3), np.float32)
+        mem = np.zeros(self.n_slices * max(self.n_vpl1, 1), np.int32)
+        cone = np.zeros((nc, 4), np.float32)
+        L.rref_ls_clusters(self.h, _ptr(cnt), _ptr(rep), _ptr(w), _ptr(up), _ptr(wi), _ptr(inc), _ptr(pdf),
+                           _ptr(size), _ptr(mem), _ptr(cone))
+        return {"count": cnt, "rep": rep, "weight": w, "upper": up, "wi": wi, "incident": inc, "pdf": pdf,
+                "size": size, "members": mem[: int(size.sum())], "cone": cone}
+
+    def maps(self):
+        ns, res = self.n_slices, self.res
+        m = np.zeros((ns, res, res), np.float32)
+        v = np.zeros(ns, np.uint8)
+        sm = np.zeros(ns, np.float32)
+        pr = np.zeros((ns, res, res), np.float32)
+        RefHarness.lib().rref_ls_maps(self.h, _ptr(m), _ptr(v), _ptr(sm), _ptr(pr))
+        return {"maps": m, "valid": v, "sum": sm, "prob": pr}
+
+    def gather(self, recv, clamp_mode, tau):
+        recv = np.ascontiguousarray(recv)
+        out = np.zeros((len(recv), 3), np.float32)
+        RefHarness.lib().rref_ls_gather(self.h, _ptr(recv), len(recv), clamp_mode, tau, _ptr(out))
+        return out
+
+
+def column_magnitudes(mat: np.ndarray) -> np.ndarray:
+    """The magnitude of every flattened column [cols][rows][3] summed in order, as
+    ClusterBuilder's magnitude() (cluster_builder.cc:14-20) computes it in float."""
+    flat = np.ascontiguousarray(mat, np.float32).reshape(mat.shape[0], -1)
+    sq = flat * flat
+    return np.sqrt(np.cumsum(sq, axis=1, dtype=np.float32)[:, -1]).astype(np.float32)
+
