@@ -442,21 +442,100 @@ def run_batch(args):
     return 0
 
 
+def run_lightslice(args):
+    """LightSlice on the scaled scene: 512 x 512 shading points, the first 32,768 VPLs (those
+    of bounce <= 1 are clustered), slices of at most 1,024 points (~256), 1,000 global
+    clusters refined to at most 2,000 per slice over 32 neighbouring slices.  Reports the
+    build stages (device reduced matrix + clustering, host refinement) and the clustered
+    gather (every pixel x its slice's clusters, one shadow ray each) timed on the device with
+    the L2 flushed between steps.  Prints one JSON line."""
+    import torch
+    from renzoku_b200 import build as rbuild
+    rbuild.build()
+    from renzoku_b200 import rzk, scenegen as sg
+    ctx = rzk.Context(0)
+    sc = sg.room_objects(2000, WIDTH, HEIGHT)
+    agg = rzk.AggregateCuda(ctx, sc)
+    cam = rzk.Camera(sc.camera)
+    recv = agg.primary(cam)
+    vt, n_made = rzk.VplGeneratorCuda(agg).spawn(VPL_SEED, VPL_PARTICLES, MAX_BOUNCE)
+    vt = vt[: N_VPL * 96].contiguous()
+    vpls_np = rzk.records_from_device(vt, sg.VPL_DTYPE)
+    _, num_emitted = select_vpls(vpls_np)
+    ev = rzk.VirtualPointLightCuda(agg, rzk.CLAMP_RADIANCE, 1.0)
+    tau = float(np.float32(0.1 * ev.mean_contribution(recv, cam.n_pixels, vt, N_VPL, seed=VPL_SEED,
+                                                       n_pairs=TAU_PAIRS)))
+    params = rzk.lightslice_params(num_clusters=1000, max_slice_size=1024, num_neighbor_slices=32,
+                                   max_slice_clusters=2000, seed=VPL_SEED)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ls = rzk.LightSliceCuda.create(agg, recv, WIDTH, HEIGHT, vt, N_VPL, params)
+    build_s = time.perf_counter() - t0
+    info = ls.info()
+    counts = ls.clusters()["count"]
+    slice_of = ls.find_slice(recv, cam.n_pixels).cpu().numpy()
+    evals = int(counts[slice_of[slice_of >= 0]].sum())
+    out = torch.empty((cam.n_pixels, 3), dtype=torch.float32, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def step():
+        ls.gather(recv, cam.n_pixels, rzk.CLAMP_RADIANCE, tau, scale=1.0 / num_emitted, out=out)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    times = []
+    with ClockSampler(0) as clk:
+        for _ in range(args.steps):
+            flush.fill_(1)
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            step()
+            b.record(stream)
+            b.synchronize()
+            times.append(a.elapsed_time(b) / 1e3)
+    ctx.check()
+    ms = 1e3 * sum(times) / len(times)
+    stages = dict(zip(["points_and_filter", "slicing", "reduced_matrix", "global_clustering",
+                       "refinement", "maps", "tables"], info["ms"][:7]))
+    line = {
+        "metric": "LightSlice clustered-gather evals/s (pixel x slice-cluster representative, shadow ray each)",
+        "value": evals / (ms / 1e3), "unit": "evals/s", "n_gpus": 1, "steps": len(times),
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "lightslice_room_objects_300k_tris_512x512_32768_vpls",
+                   "slices": info["slices"], "points": info["points"], "vpls_used": info["vpls_used"],
+                   "global_clusters": info["global_clusters"], "slice_clusters": info["slice_clusters"],
+                   "evals_per_step": evals, "max_slice_size": 1024, "num_clusters": 1000,
+                   "max_slice_clusters": 2000, "neighbor_slices": 32,
+                   "l2": "flushed between timed steps (256 MiB write)"},
+        "build_s": build_s, "build_stage_ms": stages, "clocks": clk.summary(), "gpu_launches": 7 * len(times),
+        "image_finite": bool(torch.isfinite(out).all()), "tau": tau,
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="scaled", choices=["scaled", "batch"],
+    ap.add_argument("--workload", default="scaled", choices=["scaled", "batch", "lightslice"],
                     help="scaled: the 512x512 x 32,768-VPL gather (default); batch: 64 uneven "
-                         "instances, batched + graph vs plain launches (1 GPU)")
+                         "instances, batched + graph vs plain launches (1 GPU); lightslice: "
+                         "LightSlice build + clustered gather on the scaled scene (1 GPU)")
     ap.add_argument("--instances", type=int, default=64)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "batch":
         return run_batch(args)
+    if args.workload == "lightslice":
+        return run_lightslice(args)
     return run_ours(args)
 
 
