@@ -183,6 +183,14 @@ class Camera:
     def n_pixels(self) -> int:
         return self.spec.width * self.spec.height
 
+    @property
+    def width(self) -> int:
+        return self.spec.width
+
+    @property
+    def height(self) -> int:
+        return self.spec.height
+
 
 class AggregateCuda:
     """Device-resident scene + LBVH; the Aggregate interface (aggregate.h:15-91)."""
