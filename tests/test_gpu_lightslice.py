@@ -4,8 +4,9 @@ On an all-Lambertian scene every stage is bit-exact: the 6-D points and slicing,
 reduced matrix (visibility x incident radiance), the refined clusters and maps, the slice
 lookup of every pixel and the clustered gather.  On the mixed-material scene the incident
 radiance of glossy VPLs goes through CUDA's powf / expf, so the stages after the reduced
-matrix are compared on the device's own matrix: clusters and maps stay bit-exact, and the
-gather (glossy BRDFs at both ends) matches to a relative L2 error below 1e-5.
+matrix are compared on the device's own matrix: the clusters stay bit-exact (their incident
+totals, which the reference recomputes on the host, within 1e-5), and the gather (glossy
+BRDFs at both ends) matches to a relative L2 error below 1e-5.
 """
 import numpy as np
 import pytest
@@ -95,8 +96,10 @@ def test_lightslice_mixed_materials(ctx, oracle_built):
     assert np.allclose(R, R_ref, rtol=1e-5, atol=1e-12)
     _refine_ref_on(rls, ref, ls, R, V)
     ca, cb = ls.clusters(), rls.clusters()
-    for key in ("count", "size", "members", "rep", "weight", "upper", "wi", "incident", "pdf"):
+    for key in ("count", "size", "members", "rep", "weight", "upper", "wi", "pdf"):
         assert np.array_equal(ca[key], cb[key]), key
+    # the reference recomputes each member's incident radiance with the host's powf / expf
+    assert np.allclose(ca["incident"], cb["incident"], rtol=1e-5, atol=1e-12)
     recv_np = rzk.records_from_device(recv, sg.RECEIVER_DTYPE)
     for mode, tau in ((rzk.CLAMP_NONE, 0.0), (rzk.CLAMP_FORM_FACTOR, 1e-3)):
         out = ls.gather(recv, cam.n_pixels, mode, tau, scale=1.0).cpu().numpy()
