@@ -22,6 +22,8 @@
  * drags in the closed LibImportance headers, so their few lines are repeated here
  * calling the reference's own Aggregate, FormFactor, Material and RadianceTerms.
  */
+#include <iostream>
+
 #include "ref_common.h"
 
 using namespace rref;
@@ -147,9 +149,15 @@ struct RefCameraDesc {
 };
 
 void *rref_create(const rzk_scene_desc *d, const RefCameraDesc *cd, uint32_t seed) {
-    Log::info().set_enable(false);
-    Log::warn().set_enable(false);
-    Log::debug().set_enable(false);
+    {   // Log::info() etc. print their level tag before returning the stream: keep those
+        // tags off stdout, where callers print their own results
+        std::streambuf *sb = std::cout.rdbuf(nullptr);
+        Log::info().set_enable(false);
+        Log::warn().set_enable(false);
+        Log::debug().set_enable(false);
+        std::cout.rdbuf(sb);
+        std::cout.clear();
+    }
     RefScene *s = new RefScene();
     s->shapes = new Shapes();
     s->materials = new Materials();
