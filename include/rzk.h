@@ -339,6 +339,27 @@ rzk_status rzk_lightslice_host_find(const rzk_lightslice *ls, const float *h_poi
 rzk_status rzk_lightslice_gather(rzk_lightslice *ls, const rzk_receiver *d_recv, int n_recv, int clamp_mode,
                                  float tau, float scale, float *d_rgb, void *stream);
 
+/* Guided path tracing ---------------------------------------------------------------- */
+
+typedef struct {
+    int32_t spp;              /* samples per pixel (pixel-centre primary rays) */
+    int32_t max_bounce;       /* VirtualPointLight max_bounce, 1..16 */
+    int32_t rr_depth;         /* Russian roulette at vertices deeper than this; 0 = off */
+    float rr_prob;            /* survival probability when Russian roulette applies */
+    int32_t direct_lighting;  /* Integrator::is_direct_lighting */
+    uint32_t seed;            /* sample s of pixel k draws from stream (seed, 6, k * spp + s) */
+} rzk_guided_params;
+
+/* VirtualPointLight::guided_path_trace / trace_wellington with METRO_RANDOM
+ * (vpl.cc:907-1040) guided by a LightSlice's Jensen maps (LightSlice::sample / pdf with
+ * sampling_type JENSEN, lightslice.cc:1569-2056, 2313-2377) and FirstBounce::radiance for
+ * direct light (first_bounce.h:54-71, area_light.cc:48-142).  Russian roulette (rr_depth,
+ * rr_prob) has no reference counterpart: the reference recursion always runs to
+ * max_bounce.  Writes the per-pixel mean over spp (d_rgb [W*H][3]) and optionally every
+ * path's radiance (d_paths [W*H*spp][3], path = pixel * spp + sample). */
+rzk_status rzk_guided_render(rzk_context *ctx, rzk_scene *scene, rzk_lightslice *ls, const rzk_camera *camera,
+                             const rzk_guided_params *params, float *d_rgb, float *d_paths, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -277,6 +277,7 @@ class RefHarness:
             L.rref_ls_clusters.argtypes = [P, P, P, P, P, P, P, P, P, P, P]
             L.rref_ls_maps.argtypes = [P, P, P, P, P]
             L.rref_ls_gather.argtypes = [P, P, I32, I32, F32, P]
+            L.rref_ls_guided.argtypes = [P, P, I32, I32, I32, I32, F32, I32, U32, P]
             cls._lib = L
         return cls._lib
 
@@ -478,10 +479,17 @@ class RefLightSlice:
         return out
 
 
+    def guided(self, pixels, spp, max_bounce, rr_depth=0, rr_prob=1.0, direct=True, seed=2013):
+        """Per-path radiance [len(pixels)][spp][3] of the reference's guided path tracer."""
+        pixels = np.ascontiguousarray(pixels, np.int32)
+        out = np.zeros((len(pixels), spp, 3), np.float32)
+        RefHarness.lib().rref_ls_guided(self.h, _ptr(pixels), len(pixels), spp, max_bounce, rr_depth, rr_prob,
+                                        1 if direct else 0, seed, _ptr(out))
+        return out
+
 def column_magnitudes(mat: np.ndarray) -> np.ndarray:
     """The magnitude of every flattened column [cols][rows][3] summed in order, as
     ClusterBuilder's magnitude() (cluster_builder.cc:14-20) computes it in float."""
     flat = np.ascontiguousarray(mat, np.float32).reshape(mat.shape[0], -1)
     sq = flat * flat
     return np.sqrt(np.cumsum(sq, axis=1, dtype=np.float32)[:, -1]).astype(np.float32)
-

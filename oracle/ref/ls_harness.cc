@@ -76,6 +76,7 @@
 #undef private
 #undef protected
 #include "lightslice.cc"
+#include "first_bounce.h"
 
 using namespace rref;
 
@@ -448,6 +449,85 @@ void rref_ls_maps(void *hp, float *maps, uint8_t *valid, float *sum, float *prob
             }
         valid[s] = ls->sampling_records[s].is_valid ? 1 : 0;
         sum[s] = ls->sampling_records[s].sum_vpl;
+    }
+}
+
+/* VirtualPointLight::trace_wellington with METRO_RANDOM (vpl.cc:934-1040), restated (it
+ * is a VirtualPointLight member) around the reference's FirstBounce::radiance,
+ * ShadingGeometry, Material and LightSlice::sample / pdf; plus the Russian roulette
+ * extension at vertices deeper than rr_depth (0 = off). */
+static Rgb ref_trace(RefLs *h, const Receiver &r, int bounce, int max_bounce, int rr_depth, float rr_prob,
+                     bool direct) {
+    Scene *scene = h->ls->scene;
+    Aggregate *agg = scene->get_aggregate();
+    Random &rd = *scene->get_random();
+    Float tmin = scene->get_tmin(), max_tmax = scene->get_max_tmax(), tick = scene->get_tick();
+    if (bounce > max_bounce) return DefaultRgb::black;
+    if (r.light) {
+        if (bounce == 1 && direct) {
+            Rgb Le;
+            r.light->query(r.p, r.shading_n, r.wo, Le);
+            return Le;
+        }
+        return DefaultRgb::black;
+    }
+    LocalGeometry dg(r);
+    ShadingGeometry sg(r);
+    HitRecord rec;
+    Vec3 wi;
+    Float pdf_wi;
+    Rgb radiance, brdf;
+    bool is_brdf_sampling = rd() < 0.5f;
+    if (bounce > 1 || (bounce == 1 && direct)) radiance = FirstBounce::radiance(scene, r, NULL);
+    if (bounce >= max_bounce) return radiance;
+    bool rr = false;
+    if (rr_depth > 0 && bounce > rr_depth) {
+        if (rd() >= rr_prob) return radiance;
+        rr = true;
+    }
+    if (is_brdf_sampling) brdf = sg.sample(rd, wi, pdf_wi);
+    else brdf = h->ls->sample(rd, r, wi, pdf_wi);
+    if (pdf_wi > 0.0f) {
+        Ray ray(r.p, wi);
+        if (agg->hit(ray, tmin, max_tmax, tick, rec)) {
+            if (rec.light) return radiance;
+            Receiver recv(ray, rec);
+            Rgb Li = ref_trace(h, recv, bounce + 1, max_bounce, rr_depth, rr_prob, direct);
+            Float pdf_wi_other;
+            if (is_brdf_sampling) pdf_wi_other = h->ls->pdf(r, wi);
+            else pdf_wi_other = r.m->pdf(dg, r.wo, wi);
+            Float weight = pdf_wi / (pdf_wi + pdf_wi_other);
+            Rgb term = weight * Li * brdf * sg.cosine(wi) / pdf_wi * 2;
+            if (rr) term = term / rr_prob;
+            radiance += term;
+        }
+    }
+    return radiance;
+}
+
+/* Guided path tracing of the given pixels (VirtualPointLight::guided_path_trace,
+ * vpl.cc:907-932, pixel-centre rays): sample s of pixel k from the stream
+ * (seed, 6, k * spp + s); out[(i * spp + s) * 3] for the i-th listed pixel. */
+void rref_ls_guided(void *hp, const int32_t *pixels, int n, int spp, int max_bounce, int rr_depth, float rr_prob,
+                    int direct, uint32_t seed, float *out) {
+    RefLs *h = (RefLs *)hp;
+    LightSlice *ls = h->ls;
+    ls->sampling_type = LightSlice::LocalSampler::JENSEN;
+    Scene *scene = ls->scene;
+    Size2 img = scene->get_image_size();
+    for (int i = 0; i < n; ++i) {
+        const int k = pixels[i];
+        for (int smp = 0; smp < spp; ++smp) {
+            rref_rng_stream(seed, 6u, (uint32_t)(k * spp + smp));
+            Ray r = scene->get_camera()->shoot_ray(k / (int)img.width, k % (int)img.width);
+            HitRecord rec;
+            Rgb L;
+            if (scene->get_aggregate()->hit(r, scene->get_tmin(), scene->get_max_tmax(), scene->get_tick(), rec)) {
+                Receiver recv(r, rec);
+                L = ref_trace(h, recv, 1, max_bounce, rr_depth, rr_prob, direct != 0);
+            }
+            put3(out + 3 * ((size_t)i * spp + smp), L);
+        }
     }
 }
 

@@ -30,7 +30,7 @@ constexpr int kWideEmpty = 0x7fffffff;
 // Area light as the VPL generator samples it (area_light.cc:27-46, quad.cc:73-87).
 struct DevLight {
     float4 p0[2], p1[2], p2[2];   // the (one or two) triangles of the light's shape
-    float4 n[2];                  // their facet normals; .w = 1/area
+    float4 n[2];                  // their facet normals; .w = area
     float4 basis_n, basis_u;      // Surface::get_basis: larger triangle's n and tangent
     float4 emit;                  // radiance; .w unused
     float t0_ratio;

@@ -14,6 +14,7 @@
 // Random streams (seed, stream, path): kd-tree + slice representatives (seed, 4, 0), global
 // clustering (seed, 1, 0), refinement of slice s (seed, 5, s).
 #include "rzk_gather_dev.cuh"
+#include "rzk_guide.cuh"
 #include "rzk_hostutil.h"
 #include "rzk_cluster.cuh"
 
@@ -35,22 +36,6 @@ constexpr float kPlaneBias = -1e-3f;              // KdTreeN::PLANE_BIAS (kdtree
 constexpr float kPi = 3.14159265358979f;          // common.h:38-41
 constexpr float kTwoPi = 6.28318530717959f;
 constexpr float kZeroEps = 1e-6f;                 // ZERO_EPSILON (common.h:55)
-
-// map_vec6 (lightslice.cc:148-190): position, and the reflection direction (glossy) or the
-// normal (diffuse) scaled by diagonal / 16.
-__host__ __device__ inline void map_vec6(V3 p, V3 n, const rzk_material *m, V3 wo, float diag, float *out) {
-    const float weight = 1.0f / 16.0f * diag;
-    V3 d = n;
-    if (m && (m->type == RZK_BSDF_PHONG || m->type == RZK_BSDF_WARD)) {
-        // ISpecular::get_gloss_exponential (phong.h:49-51, ward.h:38-40)
-        const float g = m->type == RZK_BSDF_PHONG ? m->p0 : smax(1.0f / m->p0, 1.0f / m->p1);
-        V3 wr = sub(scl(n, 2.0f * dot(wo, n)), wo);
-        const float gs = smin(4.0f, smax(1.0f, g / 1000.0f));
-        d = scl(wr, gs);
-    }
-    out[0] = p.x; out[1] = p.y; out[2] = p.z;
-    out[3] = d.x * weight; out[4] = d.y * weight; out[5] = d.z * weight;
-}
 
 // LightSlice::generate_slices (lightslice.cc:261-275): a point per pixel hit with a material.
 __global__ void points_kernel(const rzk_receiver *recv, int n, const rzk_material *mats, float diag,
@@ -624,6 +609,10 @@ struct rzk_lightslice {
     DBuf<rzk_vpl> d_reps;
     DBuf<float> d_weights;
     DBuf<int> d_rep_off, d_rep_cnt;
+    // device copy of the sampling state for the guided path tracer (built on first use)
+    bool guide_ready = false;
+    DBuf<float> g_box, g_rep, g_uvn, g_prob, g_row_cdf, g_col_cdf, g_total;
+    DBuf<uint8_t> g_valid;
     // per-gather scratch (grown on demand)
     DBuf<int> d_slice, d_count, d_off, d_cursor, d_pix, d_tile_off, d_work;
     DBuf<rzk_receiver> d_perm;
@@ -1038,6 +1027,67 @@ int cluster_gather_grid() {
 }
 
 }  // namespace
+
+rzk_status rzk::guide_tables(rzk_lightslice *L, GuideDev *out, cudaStream_t st) {
+    if (!L || !L->on_device || !out) return RZK_ERR_INVALID;
+    const int ns = (int)L->kd.clusters.size(), res = L->prm.map_resolution;
+    if (!L->guide_ready) {
+        std::vector<float> box(12 * (size_t)ns), rep(3 * (size_t)ns), uvn(9 * (size_t)ns);
+        std::vector<float> prob((size_t)ns * res * res);
+        for (int s = 0; s < ns; ++s) {
+            for (int d = 0; d < 6; ++d) {
+                box[12 * (size_t)s + d] = L->kd.boxes[s].mn[d];
+                box[12 * (size_t)s + 6 + d] = L->kd.boxes[s].mx[d];
+            }
+            for (int d = 0; d < 3; ++d) rep[3 * (size_t)s + d] = L->kd.data[L->rep_point[s]].p[d];
+            const rzk_receiver &rv = L->rep_recv[s];
+            for (int d = 0; d < 3; ++d) {
+                uvn[9 * (size_t)s + d] = rv.u[d];
+                uvn[9 * (size_t)s + 3 + d] = rv.v[d];
+                uvn[9 * (size_t)s + 6 + d] = rv.n[d];
+            }
+            // DiscretePdf2D::probability (pdf.cc:188-193)
+            for (int k = 0; k < res * res; ++k)
+                prob[(size_t)s * res * res + k] = L->maps[(size_t)s * res * res + k] / L->map_total[s];
+        }
+        LS_TRY(L->g_box.alloc(box.size()));
+        LS_TRY(L->g_rep.alloc(rep.size()));
+        LS_TRY(L->g_uvn.alloc(uvn.size()));
+        LS_TRY(L->g_prob.alloc(prob.size()));
+        LS_TRY(L->g_row_cdf.alloc(L->map_row_cdf.size()));
+        LS_TRY(L->g_col_cdf.alloc(L->map_cdf_col.size()));
+        LS_TRY(L->g_total.alloc(ns));
+        LS_TRY(L->g_valid.alloc(ns));
+        LS_TRY(cudaMemcpyAsync(L->g_box.p, box.data(), sizeof(float) * box.size(), cudaMemcpyHostToDevice, st));
+        LS_TRY(cudaMemcpyAsync(L->g_rep.p, rep.data(), sizeof(float) * rep.size(), cudaMemcpyHostToDevice, st));
+        LS_TRY(cudaMemcpyAsync(L->g_uvn.p, uvn.data(), sizeof(float) * uvn.size(), cudaMemcpyHostToDevice, st));
+        LS_TRY(cudaMemcpyAsync(L->g_prob.p, prob.data(), sizeof(float) * prob.size(), cudaMemcpyHostToDevice, st));
+        LS_TRY(cudaMemcpyAsync(L->g_row_cdf.p, L->map_row_cdf.data(), sizeof(float) * L->map_row_cdf.size(),
+                               cudaMemcpyHostToDevice, st));
+        LS_TRY(cudaMemcpyAsync(L->g_col_cdf.p, L->map_cdf_col.data(), sizeof(float) * L->map_cdf_col.size(),
+                               cudaMemcpyHostToDevice, st));
+        LS_TRY(cudaMemcpyAsync(L->g_total.p, L->map_total.data(), sizeof(float) * ns, cudaMemcpyHostToDevice, st));
+        LS_TRY(cudaMemcpyAsync(L->g_valid.p, L->valid.data(), ns, cudaMemcpyHostToDevice, st));
+        LS_TRY(cudaStreamSynchronize(st));
+        L->guide_ready = true;
+    }
+    GuideDev &G = *out;
+    G.kd = L->d_kd.p;
+    G.box = L->g_box.p;
+    G.rep_pos = L->g_rep.p;
+    G.rec_uvn = L->g_uvn.p;
+    G.rec_valid = L->g_valid.p;
+    G.prob = L->g_prob.p;
+    G.row_cdf = L->g_row_cdf.p;
+    G.col_cdf = L->g_col_cdf.p;
+    G.total = L->g_total.p;
+    G.n_kd = L->n_kd;
+    G.n_slices = ns;
+    G.res = res;
+    G.view_cos = std::cos(kPi * 0.25f);   // view_similarity_cosine_max (lightslice.cc:70)
+    G.diag = L->diag;
+    return RZK_OK;
+}
 
 extern "C" {
 

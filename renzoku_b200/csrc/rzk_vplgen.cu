@@ -8,116 +8,13 @@
 // depend on how many particles run or in which order.  Each particle writes up to
 // max_bounce - 1 VPLs into its own slots; an exclusive scan of the per-particle counts
 // then compacts them into the reference's push order (particle-major, bounce-minor).
-#include "rzk_traverse.cuh"
+#include "rzk_sample.cuh"
 
 namespace rzk {
 
 namespace {
 
 constexpr int kGenBlock = 128;
-
-// Phong / Ward sampling weights (phong.cc:6-16, ward.cc:15-24): Rgb::max of kd and ks,
-// normalised by their sum.
-__device__ __forceinline__ void rho_terms(const rzk_material &m, float &rho_d, float &rho_s) {
-    float rd = m.kd[0]; if (m.kd[1] > rd) rd = m.kd[1]; if (m.kd[2] > rd) rd = m.kd[2];
-    float rs = m.ks[0]; if (m.ks[1] > rs) rs = m.ks[1]; if (m.ks[2] > rs) rs = m.ks[2];
-    float total = rd + rs;
-    if (total > 0.0f) { rd /= total; rs /= total; }
-    rho_d = rd; rho_s = rs;
-}
-
-// Phong / Ward / Lambertian pdf (lambertian.cc:70-75, phong.cc:89-103, ward.cc:118-134)
-__device__ float brdf_pdf(const rzk_material &m, const Onb &uvn, V3 wo, V3 wi, float rho_d, float rho_s) {
-    if (dot(wi, uvn.n) <= ZERO_EPSILON || dot(wo, uvn.n) <= ZERO_EPSILON) return 0.0f;
-    if (m.type == RZK_BSDF_LAMBERTIAN) return dot(uvn.n, wi) * INV_PI;
-    if (m.type == RZK_BSDF_PHONG) {
-        float n = m.p0;
-        V3 nn = uvn.n;
-        float pdf = rho_d * (dot(nn, wi) * INV_PI);
-        V3 wr = sub(scl(nn, 2 * dot(wi, nn)), wi);
-        float ca = dot(wo, wr);
-        if (ca > 0.0f) pdf += rho_s * (n + 1) * INV_2PI * powf(ca, n);
-        return pdf;
-    }
-    float ax = m.p0, ay = m.p1;
-    float ax2 = ax * ax, ay2 = ay * ay;
-    float inv4 = 1.0f / (4 * A_PI * ax * ay);
-    float z = dot(uvn.n, wi);
-    V3 wh = unit(w2l(uvn, add(wi, wo)));
-    float expo = expf(-(wh.x * wh.x / ax2 + wh.y * wh.y / ay2) / (wh.z * wh.z));
-    float ct = wh.z;
-    V3 lwo = unit(w2l(uvn, wo));
-    float ct3 = ct * ct * ct;
-    return rho_d * (z * INV_PI) + rho_s * (inv4 / (dot(wh, lwo) * ct3) * expo);
-}
-
-__device__ Rgb brdf_sample(const rzk_material &m, const Onb &uvn, V3 wo, Rng &g, V3 &wi, float &pdf) {
-    if (dot(wo, uvn.n) <= ZERO_EPSILON) { wi = mk(0, 0, 0); pdf = 0.0f; return crgb(0, 0, 0); }
-    if (m.type == RZK_BSDF_LAMBERTIAN) {
-        float sx = g.uniform(), sy = g.uniform();
-        float phi = TWO_PI * sx;
-        float sin_theta = sqrtf(sy);
-        float x = sin_theta * cosf(phi);
-        float y = sin_theta * sinf(phi);
-        float z = sqrtf(1 - sin_theta * sin_theta);
-        wi = unit(l2w(uvn, mk(x, y, z)));
-        pdf = z * INV_PI;
-        return cscl(crgb(m.kd[0], m.kd[1], m.kd[2]), INV_PI);
-    }
-    float rho_d, rho_s;
-    rho_terms(m, rho_d, rho_s);
-    float eps = g.uniform();
-    if (eps < rho_d) {
-        float sx = g.uniform(), sy = g.uniform();
-        float phi = TWO_PI * sx;
-        float sin_theta = sqrtf(sy);
-        float x = sin_theta * cosf(phi);
-        float y = sin_theta * sinf(phi);
-        float z = sqrtf(1.0f - sin_theta * sin_theta);
-        wi = unit(l2w(uvn, mk(x, y, z)));
-    } else if (m.type == RZK_BSDF_PHONG) {
-        float sx = g.uniform(), sy = g.uniform();
-        Onb o = onb_from_nu(wo, uvn.n);
-        float phi = TWO_PI * sx;
-        float alpha = acosf(powf(sy, 1.0f / (m.p0 + 1)));
-        float st_ = sinf(alpha), ct_ = cosf(alpha), sp = sinf(phi), cp = cosf(phi);
-        V3 wr = l2w(o, mk(st_ * cp, st_ * sp, ct_));
-        V3 nn = uvn.n;
-        float d = dot(wr, nn);
-        if (d < 0.0f) { wi = mk(0, 0, 0); pdf = 0.0f; return crgb(0, 0, 0); }
-        wi = sub(scl(nn, 2 * d), wr);
-    } else {
-        // Vec2 sampler(rd.rand_exclude_01(), rd.rand_exclude_01()) (ward.cc:58) as the
-        // reference's compiler evaluates it: right to left, the second coordinate first.
-        float sy = g.uniform_ex01();
-        float sx = g.uniform_ex01();
-        float ax = m.p0, ay = m.p1;
-        float ax2 = ax * ax, ay2 = ay * ay, ay_ax = ay / ax;
-        V3 lwo = unit(w2l(uvn, wo));
-        float angle = TWO_PI * sx;
-        float phi = atanf(ay_ax * tanf(angle));
-        if (sinf(phi) * sinf(angle) < 0 || cosf(phi) * cosf(angle) < 0) phi += A_PI;
-        float cp = cosf(phi), sp = sinf(phi);
-        float theta = atanf(sqrtf(-logf(sy) / (cp * cp / ax2 + sp * sp / ay2)));
-        float st_ = sinf(theta), ct_ = cosf(theta);
-        V3 wh = mk(st_ * cp, st_ * sp, ct_);
-        V3 lwi = sub(scl(wh, 2 * dot(lwo, wh)), lwo);
-        wi = l2w(uvn, lwi);
-    }
-    pdf = brdf_pdf(m, uvn, wo, wi, rho_d, rho_s);
-    return brdf_eval(m, uvn, wo, wi);
-}
-
-__device__ __forceinline__ rzk_material ld_mat(const rzk_material *m) { return *m; }
-
-template <int STRIDE>
-__device__ __forceinline__ bool trace_closest(const DevScene &s, const Ray &r, Stack<STRIDE> &stk, HitGeo &h) {
-    float t, b, g;
-    int slot = closest_hit<STRIDE>(s, r, s.tmin, RAY_TMAX, stk, &t, &b, &g);
-    if (slot < 0) return false;
-    fill_hit(s, r, slot, t, b, g, h);
-    return true;
-}
 
 __device__ __forceinline__ void store_vpl(rzk_vpl *o, const HitGeo &h, V3 wi, Rgb c, int bounce, int path) {
     float w[24];

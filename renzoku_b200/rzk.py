@@ -81,6 +81,7 @@ SIGNATURES = [
     ("rzk_lightslice_host_refine", I32, [P, P, P, I32, P, P, I32, P, P, P, P]),
     ("rzk_lightslice_host_find", I32, [P, P, I32, P]),
     ("rzk_lightslice_gather", I32, [P, P, I32, I32, F32, F32, P, P]),
+    ("rzk_guided_render", I32, [P, P, P, P, P, P, P, P]),
 ]
 
 _LIB = None
@@ -457,6 +458,12 @@ def lightslice_params(**kw) -> LightSliceParamsC:
     return p
 
 
+class GuidedParamsC(ctypes.Structure):
+    """ctypes mirror of rzk_guided_params."""
+    _fields_ = [("spp", I32), ("max_bounce", I32), ("rr_depth", I32), ("rr_prob", F32),
+                ("direct_lighting", I32), ("seed", U32)]
+
+
 class LightSliceCuda:
     """LightSlice (lightslice.cc): slicing, reduced matrix, clustering, per-slice refinement and
     maps built from an image's receivers and a VPL set; gather() is gather_clusters for every
@@ -581,6 +588,21 @@ class LightSliceCuda:
         check(self.lib.rzk_lightslice_gather(self.h, _dptr(recv), n_recv, clamp_mode, tau, scale, _dptr(out),
                                              _stream_ptr(stream)), "rzk_lightslice_gather")
         return out
+
+    def guided_render(self, cam: "Camera", spp: int, max_bounce: int, rr_depth: int = 0, rr_prob: float = 1.0,
+                      direct: bool = True, seed: int = 2013, paths: bool = False, out=None, stream=None):
+        """LightSlice-guided path tracing (rzk_guided_render): the per-pixel mean image, and the
+        per-path radiance [W*H, spp, 3] when paths=True."""
+        torch = _torch()
+        n = cam.n_pixels
+        if out is None:
+            out = torch.empty((n, 3), dtype=torch.float32, device="cuda")
+        pt = torch.empty((n, spp, 3), dtype=torch.float32, device="cuda") if paths else None
+        prm = GuidedParamsC(spp, max_bounce, rr_depth, rr_prob, 1 if direct else 0, seed)
+        check(self.lib.rzk_guided_render(self.agg.ctx.h, self.agg.h, self.h, cam.rec.ctypes.data, ctypes.byref(prm),
+                                         _dptr(out), _dptr(pt) if pt is not None else None, _stream_ptr(stream)),
+              "rzk_guided_render")
+        return (out, pt) if paths else out
 
     def close(self):
         if getattr(self, "h", None):

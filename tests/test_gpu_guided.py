@@ -1,0 +1,73 @@
+"""LightSlice-guided path tracing on the device against the reference's tracer.
+
+Both sides draw sample s of pixel k from the same counter-based stream (seed, 6, k * spp + s)
+and run from the same LightSlice state (slices, refined clusters, Jensen maps), so each path
+is the reference's path: the direct-light estimate (one light sample, one BRDF sample,
+balance heuristic), the one-sample choice between BRDF and map sampling, the continuation.
+They differ only where CUDA's sinf / cosf / acosf / powf / atan2f round differently from
+glibc's, which perturbs directions by ulps: nearly all paths agree to 1e-4 and the few that
+branch differently (a grazing hit, a roulette draw on the other side of a threshold) move
+the image mean by far less than its noise.
+"""
+import numpy as np
+import pytest
+
+from renzoku_b200 import scenegen as sg
+
+pytestmark = pytest.mark.gpu
+SEED = 2013
+
+
+def _setup(ctx, sc, slice_size=64, k=8, n_clusters=40, max_sc=80):
+    import torch
+    from oracle import RefHarness, column_magnitudes
+    from renzoku_b200 import rzk
+    agg = rzk.AggregateCuda(ctx, sc)
+    cam = rzk.Camera(sc.camera)
+    recv = agg.primary(cam)
+    vt, n = rzk.VplGeneratorCuda(agg).spawn(SEED, 400, 3)
+    params = rzk.lightslice_params(max_slice_size=slice_size, num_neighbor_slices=k, num_clusters=n_clusters,
+                                   max_slice_clusters=max_sc, seed=SEED, n_threads=4)
+    ls = rzk.LightSliceCuda.create(agg, recv, cam.width, cam.height, vt, n, params)
+    torch.cuda.synchronize()
+    ref = RefHarness(sc)
+    rls = ref.lightslice(slice_size, k, SEED)
+    R, V, _ = ls.matrix()
+    R, V = R.cpu().numpy(), V.cpu().numpy()
+    rls.reduced_matrix(rzk.records_from_device(vt, sg.VPL_DTYPE))
+    _, g_rep, g_w, assign = ref.cluster_by_sampling(R, n_clusters, SEED)
+    rls.refine(R, V, g_rep, g_w, assign, column_magnitudes(R), max_sc, SEED)
+    return agg, cam, ls, rls
+
+
+@pytest.mark.parametrize("rr_depth", [0, 3])
+def test_guided_paths_match_reference(ctx, oracle_built, rr_depth):
+    from oracle import RefHarness
+    if not RefHarness.available():
+        pytest.skip("reference harness not built")
+    sc = sg.room_boxes(32, 32)
+    agg, cam, ls, rls = _setup(ctx, sc)
+    spp, mb = 4, 8
+    img, paths = ls.guided_render(cam, spp, mb, rr_depth=rr_depth, rr_prob=0.5, seed=SEED, paths=True)
+    ctx.check()
+    img, paths = img.cpu().numpy(), paths.cpu().numpy()
+    assert np.isfinite(img).all() and img.sum() > 0
+    assert np.allclose(img, paths.mean(axis=1), rtol=1e-6, atol=1e-7)
+    pix = np.arange(0, cam.n_pixels, 3)
+    ref = rls.guided(pix, spp, mb, rr_depth=rr_depth, rr_prob=0.5, seed=SEED)
+    ours = paths[pix]
+    scale = np.maximum(np.abs(ref).max(axis=2), 1e-3)
+    close = (np.abs(ours - ref).max(axis=2) <= 1e-4 * scale + 1e-6)
+    assert close.mean() > 0.95, close.mean()
+    m_ref, m_ours = ref.mean(axis=(0, 1)), ours.mean(axis=(0, 1))
+    assert np.allclose(m_ours, m_ref, rtol=0.02), (m_ours, m_ref)
+
+
+def test_guided_rejects_bad_parameters(ctx):
+    import ctypes
+    from renzoku_b200 import rzk
+    lib = rzk.load()
+    prm = rzk.GuidedParamsC(0, 8, 0, 1.0, 1, 1)
+    cam = np.zeros(1, sg.CAMERA_DTYPE)
+    assert lib.rzk_guided_render(ctx.h, None, None, cam.ctypes.data, ctypes.byref(prm), None, None,
+                                 None) == rzk.ERR_INVALID
