@@ -543,7 +543,7 @@ def run_guided(args):
             break
         particles *= 2
     vt = vt[: n_vpl * 96].contiguous()
-    params = rzk.lightslice_params(num_clusters=4096, max_slice_size=1024, num_neighbor_slices=32,
+    params = rzk.lightslice_params(num_clusters=4096, max_slice_size=args.slice_size, num_neighbor_slices=32,
                                    max_slice_clusters=args.max_slice_clusters, seed=VPL_SEED)
     ls = rzk.LightSliceCuda.create(agg, recv, side, side, vt, n_vpl, params)
     torch.cuda.synchronize()
@@ -583,6 +583,7 @@ def run_guided(args):
                    "triangles": agg.n_tris, "spp": spp, "max_bounce": 8, "rr_depth": 3, "rr_prob": 0.5,
                    "vpls": n_vpl, "vpls_used": info["vpls_used"], "global_clusters": info["global_clusters"],
                    "slices": info["slices"], "slice_clusters": info["slice_clusters"], "map_resolution": 32,
+                   "max_slice_size": args.slice_size,
                    "l2": "flushed between timed steps (256 MiB write)"},
         "setup_s": setup_s, "lightslice_stage_ms": info["ms"][:7], "clocks": clk.summary(),
         "gpu_launches": len(times), "image_finite": bool(torch.isfinite(out).all()),
@@ -606,6 +607,7 @@ def main():
     ap.add_argument("--spp", type=int, default=16)
     ap.add_argument("--side", type=int, default=1024)
     ap.add_argument("--max-slice-clusters", type=int, default=4096)
+    ap.add_argument("--slice-size", type=int, default=4096)
     ap.add_argument("--instances", type=int, default=64)
     args = ap.parse_args()
     if args.impl == "reference":

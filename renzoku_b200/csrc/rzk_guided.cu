@@ -124,6 +124,7 @@ __device__ Rgb trace_path(const DevScene &s, const GuideDev &G, const PtParams &
             if (bounce == 1 && P.direct) value = light_query(s.lights[light], r.p, r.ns, r.wo);
             break;
         }
+        if (r.mat < 0) { value = crgb(0.0f, 0.0f, 0.0f); break; }   // a surface without a material
         const rzk_material m = *(s.mats + r.mat);
         const bool is_brdf = g.uniform() < 0.5f;
         Rgb radiance = crgb(0.0f, 0.0f, 0.0f);
