@@ -360,6 +360,60 @@ typedef struct {
 rzk_status rzk_guided_render(rzk_context *ctx, rzk_scene *scene, rzk_lightslice *ls, const rzk_camera *camera,
                              const rzk_guided_params *params, float *d_rgb, float *d_paths, void *stream);
 
+/* Serving ---------------------------------------------------------------------------- */
+
+enum { RZK_REQ_GATHER = 0, RZK_REQ_GUIDED = 1 };
+
+/* One request: a gather (the VPL integrator's frame, vpl.cc:496-520) or a guided render
+ * (vpl.cc:907-932) of a device-resident scene through the request's own camera. */
+typedef struct {
+    int32_t kind;                 /* RZK_REQ_GATHER or RZK_REQ_GUIDED */
+    rzk_scene *scene;
+    rzk_lightslice *lightslice;   /* guided: the scene's LightSlice */
+    rzk_camera camera;            /* the image: camera.width x camera.height pixel-centre rays */
+    const rzk_vpl *d_vpls;        /* gather: VPLs, count, clamp, 1 / num_emitted */
+    int32_t n_vpl;
+    int32_t clamp_mode;
+    float tau;
+    float scale;
+    int32_t spp;                  /* guided: as rzk_guided_params */
+    int32_t max_bounce;
+    int32_t rr_depth;
+    float rr_prob;
+    uint32_t seed;
+    float *d_rgb;                 /* caller-owned device output, width * height * 3 floats */
+} rzk_request;
+
+typedef struct {
+    int64_t hbm_budget_bytes;  /* device memory admitted requests may hold (0 = 90% of free at create) */
+    int32_t batching;          /* 1: each iteration's gathers run as one batched launch; 0: one request at a time */
+    int32_t max_batch;         /* most requests taken per iteration (0 = 256) */
+} rzk_server_params;
+
+typedef struct rzk_server rzk_server;
+
+/* A request loop with its own context, stream and worker thread on `device`.  No reference
+ * counterpart: the reference renders one scene per process (integrator_scheduler.cc). */
+rzk_status rzk_server_create(int device, const rzk_server_params *params, rzk_server **out);
+/* Finishes every admitted request, then releases the server. */
+rzk_status rzk_server_destroy(rzk_server *server);
+/* Admits the request if the device memory it will hold in flight (receivers, and for a
+ * gather its per-chunk partial sums) fits the budget next to the admitted ones, else
+ * returns RZK_ERR_BUSY without queueing it.  Thread-safe.  The caller keeps the scene, the
+ * VPLs, the LightSlice and d_rgb alive until the request is done. */
+rzk_status rzk_server_submit(rzk_server *server, const rzk_request *request, uint64_t *ticket);
+/* *state: 0 queued, 1 running, 2 done, 3 cancelled, 4 failed.  A finished request is
+ * reported once (with its latency, submit to completion) and then forgotten; the return
+ * value is the request's status. */
+rzk_status rzk_server_poll(rzk_server *server, uint64_t ticket, int32_t *state, double *latency_ms);
+/* Waits up to timeout_ms (< 0: no limit) for the request; RZK_ERR_TIMEOUT if it is still
+ * pending.  Reports and forgets it like rzk_server_poll. */
+rzk_status rzk_server_wait(rzk_server *server, uint64_t ticket, int32_t timeout_ms, double *latency_ms);
+/* Withdraws a request that is still queued; RZK_ERR_BUSY once it has been launched. */
+rzk_status rzk_server_cancel(rzk_server *server, uint64_t ticket);
+rzk_status rzk_server_stats(rzk_server *server, int64_t *submitted, int64_t *rejected, int64_t *completed,
+                            int64_t *launches, int64_t *held_bytes, int64_t *budget_bytes);
+
 #ifdef __cplusplus
 }
 #endif

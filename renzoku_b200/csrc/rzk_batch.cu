@@ -106,37 +106,27 @@ int batch_grid() {
     return std::max(1, sms * std::max(1, per_sm));
 }
 
-}  // namespace
-
-}  // namespace rzk
-
-struct rzk_batch {
-    rzk_context *ctx = nullptr;
-    std::vector<rzk::JobTable> tables;   // one per launch; item and output offsets are per table
-    float *d_partial = nullptr;
-    int *d_work = nullptr;               // one work counter per table
-    int n_jobs = 0, variant = 0, grid = 0;
-    size_t partial_floats = 0;
-};
-
-using namespace rzk;
-
-extern "C" {
-
-int rzk_batch_variants(void) { return (int)(sizeof(kBatchVariants) / sizeof(kBatchVariants[0])); }
-
-rzk_status rzk_batch_destroy(rzk_batch *b) {
-    if (!b) return RZK_ERR_INVALID;
-    if (b->d_partial) cudaFree(b->d_partial);
-    if (b->d_work) cudaFree(b->d_work);
-    delete b;
-    return RZK_OK;
+int grid_for(int variant) {
+    switch (variant) {
+        case 0: return batch_grid<4, 32, 5>();
+        case 1: return batch_grid<4, 32, 4>();
+        case 2: return batch_grid<2, 32, 1>();
+        default: return batch_grid<4, 16, 5>();
+    }
 }
 
-rzk_status rzk_batch_create(rzk_context *ctx, const rzk_gather_job *jobs, int n_jobs, int variant, int chunk_len,
-                            rzk_batch **out) {
-    if (!ctx || !jobs || n_jobs <= 0 || !out || variant < 0 || variant >= rzk_batch_variants()) return RZK_ERR_INVALID;
-    if (chunk_len < 0 || (chunk_len % 128) != 0) return RZK_ERR_INVALID;
+}  // namespace
+
+// A batch split into launch tables: consecutive jobs go into one launch until it holds
+// kJobsPerLaunch jobs or 2^30 work items.
+struct BatchPlan {
+    std::vector<JobTable> tables;
+    size_t partial_floats = 0;
+    float *bound = nullptr;   // partial buffer the tables point into
+};
+
+rzk_status batch_plan_create(const rzk_gather_job *jobs, int n_jobs, int chunk_len, BatchPlan **out) {
+    if (!jobs || n_jobs <= 0 || !out || chunk_len < 0 || (chunk_len % 128) != 0) return RZK_ERR_INVALID;
     *out = nullptr;
     std::vector<BatchJob> h(n_jobs);
     size_t partial = 0;
@@ -177,21 +167,17 @@ rzk_status rzk_batch_create(rzk_context *ctx, const rzk_gather_job *jobs, int n_
         if ((long long)b.n_wtiles * b.n_chunks >= (1LL << 30)) return RZK_ERR_CAPACITY;
         partial += 3ull * b.n_recv * b.n_chunks;
     }
-    rzk_batch *bt = new rzk_batch();
-    bt->ctx = ctx;
-    bt->n_jobs = n_jobs;
-    bt->variant = variant;
-    bt->partial_floats = partial;
-    // consecutive jobs go into one launch until it holds kJobsPerLaunch jobs or 2^30 items
+    BatchPlan *p = new BatchPlan();
+    p->partial_floats = partial;
     for (int i = 0; i < n_jobs; ++i) {
         long long items = (long long)h[i].n_wtiles * h[i].n_chunks;
-        if (bt->tables.empty() || bt->tables.back().n_jobs == kJobsPerLaunch ||
-            bt->tables.back().n_items + items >= (1LL << 30)) {
-            bt->tables.emplace_back();
-            JobTable &t = bt->tables.back();
+        if (p->tables.empty() || p->tables.back().n_jobs == kJobsPerLaunch ||
+            p->tables.back().n_items + items >= (1LL << 30)) {
+            p->tables.emplace_back();
+            JobTable &t = p->tables.back();
             memset(&t, 0, sizeof(t));
         }
-        JobTable &t = bt->tables.back();
+        JobTable &t = p->tables.back();
         BatchJob &b = h[i];
         b.item_begin = t.n_items;
         b.out_begin = t.n_out;
@@ -199,48 +185,96 @@ rzk_status rzk_batch_create(rzk_context *ctx, const rzk_gather_job *jobs, int n_
         t.n_out += 3LL * b.n_recv;
         t.jobs[t.n_jobs++] = b;
     }
-    auto fail = [&](cudaError_t e) {
-        set_last_cuda_error(e, "batch", __FILE__, __LINE__);
-        rzk_batch_destroy(bt);
-        return e == cudaErrorMemoryAllocation ? RZK_ERR_NOMEM : RZK_ERR_CUDA;
-    };
-    cudaError_t e = cudaMalloc((void **)&bt->d_partial, sizeof(float) * std::max<size_t>(partial, 1));
-    if (e != cudaSuccess) return fail(e);
-    size_t off = 0;
-    for (JobTable &t : bt->tables)
-        for (int i = 0; i < t.n_jobs; ++i) {
-            t.jobs[i].partial = bt->d_partial + off;
-            off += 3ull * t.jobs[i].n_recv * t.jobs[i].n_chunks;
-        }
-    if ((e = cudaMalloc((void **)&bt->d_work, sizeof(int) * bt->tables.size())) != cudaSuccess) return fail(e);
-    switch (variant) {
-        case 0: bt->grid = batch_grid<4, 32, 5>(); break;
-        case 1: bt->grid = batch_grid<4, 32, 4>(); break;
-        case 2: bt->grid = batch_grid<2, 32, 1>(); break;
-        default: bt->grid = batch_grid<4, 16, 5>(); break;
-    }
-    *out = bt;
+    *out = p;
     return RZK_OK;
 }
 
-rzk_status rzk_batch_run(rzk_batch *b, void *stream) {
-    if (!b) return RZK_ERR_INVALID;
-    cudaStream_t st = (cudaStream_t)stream;
-    RZK_CUDA_TRY(cudaMemsetAsync(b->d_work, 0, sizeof(int) * b->tables.size(), st));
-    for (size_t k = 0; k < b->tables.size(); ++k) {
-        const JobTable &t = b->tables[k];
-        int *work = b->d_work + k;
-        switch (b->variant) {
-            case 0: batch_gather_kernel<4, 32, 5><<<b->grid, 128, 0, st>>>(t, work); break;
-            case 1: batch_gather_kernel<4, 32, 4><<<b->grid, 128, 0, st>>>(t, work); break;
-            case 2: batch_gather_kernel<2, 32, 1><<<b->grid, 64, 0, st>>>(t, work); break;
-            default: batch_gather_kernel<4, 16, 5><<<b->grid, 128, 0, st>>>(t, work); break;
+void batch_plan_destroy(BatchPlan *p) { delete p; }
+size_t batch_plan_partial_floats(const BatchPlan *p) { return p->partial_floats; }
+int batch_plan_tables(const BatchPlan *p) { return (int)p->tables.size(); }
+
+rzk_status batch_plan_launch(BatchPlan *p, float *partial, int *work, int variant, int grid, cudaStream_t st) {
+    if (p->bound != partial) {
+        size_t off = 0;
+        for (JobTable &t : p->tables)
+            for (int i = 0; i < t.n_jobs; ++i) {
+                t.jobs[i].partial = partial + off;
+                off += 3ull * t.jobs[i].n_recv * t.jobs[i].n_chunks;
+            }
+        p->bound = partial;
+    }
+    if (grid <= 0) grid = grid_for(variant);
+    RZK_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(int) * p->tables.size(), st));
+    for (size_t k = 0; k < p->tables.size(); ++k) {
+        const JobTable &t = p->tables[k];
+        int *w = work + k;
+        switch (variant) {
+            case 0: batch_gather_kernel<4, 32, 5><<<grid, 128, 0, st>>>(t, w); break;
+            case 1: batch_gather_kernel<4, 32, 4><<<grid, 128, 0, st>>>(t, w); break;
+            case 2: batch_gather_kernel<2, 32, 1><<<grid, 64, 0, st>>>(t, w); break;
+            default: batch_gather_kernel<4, 16, 5><<<grid, 128, 0, st>>>(t, w); break;
         }
         RZK_CUDA_TRY(cudaGetLastError());
         batch_reduce_kernel<<<(unsigned)((t.n_out + 255) / 256), 256, 0, st>>>(t);
         RZK_CUDA_TRY(cudaGetLastError());
     }
     return RZK_OK;
+}
+
+}  // namespace rzk
+
+struct rzk_batch {
+    rzk_context *ctx = nullptr;
+    rzk::BatchPlan *plan = nullptr;
+    float *d_partial = nullptr;
+    int *d_work = nullptr;               // one work counter per table
+    int n_jobs = 0, variant = 0, grid = 0;
+};
+
+using namespace rzk;
+
+extern "C" {
+
+int rzk_batch_variants(void) { return (int)(sizeof(kBatchVariants) / sizeof(kBatchVariants[0])); }
+
+rzk_status rzk_batch_destroy(rzk_batch *b) {
+    if (!b) return RZK_ERR_INVALID;
+    if (b->d_partial) cudaFree(b->d_partial);
+    if (b->d_work) cudaFree(b->d_work);
+    if (b->plan) batch_plan_destroy(b->plan);
+    delete b;
+    return RZK_OK;
+}
+
+rzk_status rzk_batch_create(rzk_context *ctx, const rzk_gather_job *jobs, int n_jobs, int variant, int chunk_len,
+                            rzk_batch **out) {
+    if (!ctx || !jobs || n_jobs <= 0 || !out || variant < 0 || variant >= rzk_batch_variants()) return RZK_ERR_INVALID;
+    if (chunk_len < 0 || (chunk_len % 128) != 0) return RZK_ERR_INVALID;
+    *out = nullptr;
+    BatchPlan *plan = nullptr;
+    rzk_status r = batch_plan_create(jobs, n_jobs, chunk_len, &plan);
+    if (r != RZK_OK) return r;
+    rzk_batch *bt = new rzk_batch();
+    bt->ctx = ctx;
+    bt->plan = plan;
+    bt->n_jobs = n_jobs;
+    bt->variant = variant;
+    auto fail = [&](cudaError_t e) {
+        set_last_cuda_error(e, "batch", __FILE__, __LINE__);
+        rzk_batch_destroy(bt);
+        return e == cudaErrorMemoryAllocation ? RZK_ERR_NOMEM : RZK_ERR_CUDA;
+    };
+    cudaError_t e = cudaMalloc((void **)&bt->d_partial, sizeof(float) * std::max<size_t>(plan->partial_floats, 1));
+    if (e != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc((void **)&bt->d_work, sizeof(int) * plan->tables.size())) != cudaSuccess) return fail(e);
+    bt->grid = grid_for(variant);
+    *out = bt;
+    return RZK_OK;
+}
+
+rzk_status rzk_batch_run(rzk_batch *b, void *stream) {
+    if (!b) return RZK_ERR_INVALID;
+    return batch_plan_launch(b->plan, b->d_partial, b->d_work, b->variant, b->grid, (cudaStream_t)stream);
 }
 
 rzk_status rzk_batch_autotune(rzk_context *ctx, const rzk_gather_job *jobs, int n_jobs, int max_probe_jobs,

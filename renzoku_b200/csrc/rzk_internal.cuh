@@ -55,6 +55,8 @@ struct DevScene {
 
 struct Scene;
 
+struct BatchPlan;   // rzk_batch.cu: a batch of gathers split into launch tables
+
 }  // namespace rzk
 
 struct rzk_context {
@@ -125,4 +127,12 @@ size_t exclusive_scan_tmp_bytes(int n);
 rzk_status launch_matrix(const DevScene &s, const rzk_receiver *recv, int n_recv, const rzk_vpl *vpls,
                          int n_vpl, int mode, float tau, float *mat, uint8_t *vis, int kind,
                          cudaStream_t st);
+// rzk_batch.cu: plan a batch (validates jobs; no device work), then launch it on a partial
+// buffer of batch_plan_partial_floats floats and batch_plan_tables work counters; grid 0 =
+// the variant's resident grid.
+rzk_status batch_plan_create(const rzk_gather_job *jobs, int n_jobs, int chunk_len, BatchPlan **out);
+void batch_plan_destroy(BatchPlan *p);
+size_t batch_plan_partial_floats(const BatchPlan *p);
+int batch_plan_tables(const BatchPlan *p);
+rzk_status batch_plan_launch(BatchPlan *p, float *partial, int *work, int variant, int grid, cudaStream_t st);
 }  // namespace rzk

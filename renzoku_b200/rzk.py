@@ -82,6 +82,13 @@ SIGNATURES = [
     ("rzk_lightslice_host_find", I32, [P, P, I32, P]),
     ("rzk_lightslice_gather", I32, [P, P, I32, I32, F32, F32, P, P]),
     ("rzk_guided_render", I32, [P, P, P, P, P, P, P, P]),
+    ("rzk_server_create", I32, [I32, P, P]),
+    ("rzk_server_destroy", I32, [P]),
+    ("rzk_server_submit", I32, [P, P, P]),
+    ("rzk_server_poll", I32, [P, ctypes.c_uint64, P, P]),
+    ("rzk_server_wait", I32, [P, ctypes.c_uint64, I32, P]),
+    ("rzk_server_cancel", I32, [P, ctypes.c_uint64]),
+    ("rzk_server_stats", I32, [P, P, P, P, P, P, P]),
 ]
 
 _LIB = None
@@ -607,6 +614,81 @@ class LightSliceCuda:
     def close(self):
         if getattr(self, "h", None):
             self.lib.rzk_lightslice_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+REQ_GATHER, REQ_GUIDED = 0, 1
+
+
+class CameraC(ctypes.Structure):
+    """ctypes mirror of rzk_camera (80 bytes)."""
+    _fields_ = [("eye", F32 * 3), ("u", F32 * 3), ("v", F32 * 3), ("n", F32 * 3), ("focal", F32),
+                ("cop", F32 * 2), ("scale", F32 * 2), ("width", I32), ("height", I32), ("pad", I32)]
+
+
+class RequestC(ctypes.Structure):
+    """ctypes mirror of rzk_request."""
+    _fields_ = [("kind", I32), ("scene", P), ("lightslice", P), ("camera", CameraC), ("d_vpls", P),
+                ("n_vpl", I32), ("clamp_mode", I32), ("tau", F32), ("scale", F32), ("spp", I32),
+                ("max_bounce", I32), ("rr_depth", I32), ("rr_prob", F32), ("seed", U32), ("d_rgb", P)]
+
+
+class ServerParamsC(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", ctypes.c_int64), ("batching", I32), ("max_batch", I32)]
+
+
+def camera_c(cam: "Camera") -> CameraC:
+    c = CameraC()
+    ctypes.memmove(ctypes.byref(c), cam.rec.ctypes.data, ctypes.sizeof(CameraC))
+    return c
+
+
+class Server:
+    """The request loop (rzk_server_*): submit() returns a ticket or None when not admitted."""
+
+    def __init__(self, device=0, batching=True, hbm_budget_bytes=0, max_batch=0):
+        self.lib = load()
+        prm = ServerParamsC(hbm_budget_bytes, 1 if batching else 0, max_batch)
+        h = ctypes.c_void_p()
+        check(self.lib.rzk_server_create(device, ctypes.byref(prm), ctypes.byref(h)), "rzk_server_create")
+        self.h = h
+
+    def submit(self, req: RequestC):
+        t = ctypes.c_uint64()
+        st = self.lib.rzk_server_submit(self.h, ctypes.byref(req), ctypes.byref(t))
+        if st == ERR_BUSY:
+            return None
+        check(st, "rzk_server_submit")
+        return t.value
+
+    def poll(self, ticket):
+        state, lat = I32(), ctypes.c_double()
+        st = self.lib.rzk_server_poll(self.h, ticket, ctypes.byref(state), ctypes.byref(lat))
+        return state.value, (lat.value if state.value >= 2 else None), st
+
+    def wait(self, ticket, timeout_ms=-1):
+        lat = ctypes.c_double()
+        st = self.lib.rzk_server_wait(self.h, ticket, timeout_ms, ctypes.byref(lat))
+        return st, lat.value
+
+    def cancel(self, ticket):
+        return self.lib.rzk_server_cancel(self.h, ticket)
+
+    def stats(self):
+        v = [ctypes.c_int64() for _ in range(6)]
+        check(self.lib.rzk_server_stats(self.h, *[ctypes.byref(x) for x in v]), "rzk_server_stats")
+        return dict(zip(["submitted", "rejected", "completed", "launches", "held_bytes", "budget_bytes"],
+                        [x.value for x in v]))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.rzk_server_destroy(self.h)
             self.h = None
 
     def __del__(self):
