@@ -593,13 +593,132 @@ def run_guided(args):
     return 0
 
 
+def run_serve(args):
+    """Serving mix: 8 device-resident scenes (room filled to 50k-1M triangles, log-uniform,
+    seed 7), each with 100,000 VPLs and a LightSlice; Poisson arrivals (seed 8) at each rate
+    for --duration seconds; every request is a gather or a guided render (50/50) with image
+    side 64-1024, 1k-100k VPLs and 1-16 spp, log-uniform.  The same request streams run
+    through the batched server and through the one-request-at-a-time server; admission by
+    an HBM budget.  Prints one JSON line (value = p99 latency of the batched server at the
+    lowest rate)."""
+    import dataclasses
+    import math
+    import torch
+    from renzoku_b200 import build as rbuild
+    rbuild.build()
+    from renzoku_b200 import instances as im, rzk, scenegen as sg
+    ctx = rzk.Context(0)
+    rng = np.random.default_rng(7)
+    worlds = []
+    t0 = time.perf_counter()
+    for k in range(8):
+        n_tris = int(round(math.exp(rng.uniform(math.log(50_000), math.log(1_000_000)))))
+        sc = sg.room_filled(n_tris, 256, 256, 700 + k)
+        agg = rzk.AggregateCuda(ctx, sc)
+        cam = rzk.Camera(sc.camera)
+        recv = agg.primary(cam)
+        vt, emitted = im.spawn_vpls(agg, VPL_SEED + k, 100_000)
+        ev = rzk.VirtualPointLightCuda(agg, rzk.CLAMP_RADIANCE, 1.0)
+        tau = float(np.float32(0.1 * ev.mean_contribution(recv, cam.n_pixels, vt, 100_000, seed=VPL_SEED,
+                                                           n_pairs=TAU_PAIRS)))
+        ls = rzk.LightSliceCuda.create(agg, recv, 256, 256, vt, 100_000,
+                                       rzk.lightslice_params(num_clusters=1000, max_slice_size=1024,
+                                                             num_neighbor_slices=32, max_slice_clusters=1000,
+                                                             seed=VPL_SEED))
+        worlds.append({"sc": sc, "agg": agg, "vpls": vt, "emitted": emitted, "tau": tau, "ls": ls})
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t0
+    rates = [float(x) for x in args.rates.split(",")]
+    logu = lambda g, lo, hi: math.exp(g.uniform(math.log(lo), math.log(hi)))
+
+    def requests(rate):
+        g = np.random.default_rng(8 + int(rate * 1000))
+        t, out = 0.0, []
+        while True:
+            t += g.exponential(1.0 / rate)
+            if t > args.duration:
+                return out
+            side = max(64, int(round(logu(g, 64, 1024) / 8.0)) * 8)
+            out.append({"t": t, "guided": bool(g.random() < 0.5), "scene": int(g.integers(8)), "side": side,
+                        "vpls": int(round(logu(g, 1000, 100_000))), "spp": int(round(logu(g, 1, 16)))})
+
+    def make_req(d, out):
+        w = worlds[d["scene"]]
+        cam = rzk.Camera(dataclasses.replace(w["sc"].camera, width=d["side"], height=d["side"]))
+        r = rzk.RequestC()
+        r.kind = rzk.REQ_GUIDED if d["guided"] else rzk.REQ_GATHER
+        r.scene = w["agg"].h.value
+        r.lightslice = w["ls"].h.value
+        r.camera = rzk.camera_c(cam)
+        r.d_vpls = w["vpls"].data_ptr()
+        r.n_vpl = d["vpls"]
+        r.clamp_mode = rzk.CLAMP_RADIANCE
+        r.tau = w["tau"]
+        r.scale = 1.0 / w["emitted"]
+        r.spp, r.max_bounce, r.rr_depth, r.rr_prob, r.seed = d["spp"], 8, 3, 0.5, VPL_SEED
+        r.d_rgb = out.data_ptr()
+        return r
+
+    def run(batching, reqs):
+        srv = rzk.Server(0, batching=batching, hbm_budget_bytes=int(args.budget_gb * (1 << 30)))
+        pending, lat, rejected = {}, [], 0
+        t_start = time.perf_counter()
+        for d in reqs:
+            while True:
+                now = time.perf_counter() - t_start
+                if now >= d["t"]:
+                    break
+                time.sleep(min(0.002, d["t"] - now))
+            out = torch.empty((d["side"] * d["side"], 3), dtype=torch.float32, device="cuda")
+            t = srv.submit(make_req(d, out))
+            if t is None:
+                rejected += 1
+            else:
+                pending[t] = out
+            for tk in list(pending):
+                st, l, _ = srv.poll(tk)
+                if st >= 2:
+                    lat.append(l)
+                    del pending[tk]
+        for tk in list(pending):
+            _, l = srv.wait(tk)
+            lat.append(l)
+        wall = time.perf_counter() - t_start
+        stats = srv.stats()
+        srv.close()
+        lat = np.array(lat) if lat else np.zeros(1)
+        return {"completed": len(lat), "rejected": rejected, "wall_s": wall, "throughput_rps": len(lat) / wall,
+                "p50_ms": float(np.percentile(lat, 50)), "p95_ms": float(np.percentile(lat, 95)),
+                "p99_ms": float(np.percentile(lat, 99)), "launches": stats["launches"]}
+
+    sweep = []
+    for rate in rates:
+        reqs = requests(rate)
+        b = run(True, reqs)
+        p = run(False, reqs)
+        sweep.append({"rate_rps": rate, "requests": len(reqs), "batched": b, "plain": p})
+    first = sweep[0]["batched"]
+    line = {
+        "metric": f"serving p99 latency (ms) at {rates[0]:g} req/s, batched server",
+        "value": first["p99_ms"], "unit": "ms", "n_gpus": 1, "steps": len(rates), "warmup": 0,
+        "ms_per_step": first["p50_ms"], "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "serving_mix_8_scenes_50k_1M_tris", "duration_s": args.duration,
+                   "hbm_budget_gb": args.budget_gb, "rates_rps": rates,
+                   "scene_triangles": [w["agg"].n_tris for w in worlds]},
+        "sweep": sweep, "setup_s": setup_s,
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="scaled", choices=["scaled", "batch", "lightslice", "guided"],
+    ap.add_argument("--workload", default="scaled", choices=["scaled", "batch", "lightslice", "guided", "serve"],
                     help="scaled: the 512x512 x 32,768-VPL gather (default); batch: 64 uneven "
                          "instances, batched + graph vs plain launches (1 GPU); lightslice: "
                          "LightSlice build + clustered gather on the scaled scene (1 GPU); guided: "
@@ -608,6 +727,9 @@ def main():
     ap.add_argument("--side", type=int, default=1024)
     ap.add_argument("--max-slice-clusters", type=int, default=4096)
     ap.add_argument("--slice-size", type=int, default=4096)
+    ap.add_argument("--rates", default="5,20,50,200", help="serve: arrival rates (req/s)")
+    ap.add_argument("--duration", type=float, default=3.0, help="serve: seconds of arrivals per rate")
+    ap.add_argument("--budget-gb", type=float, default=4.0, help="serve: HBM admission budget")
     ap.add_argument("--instances", type=int, default=64)
     args = ap.parse_args()
     if args.impl == "reference":
@@ -618,6 +740,8 @@ def main():
         return run_lightslice(args)
     if args.workload == "guided":
         return run_guided(args)
+    if args.workload == "serve":
+        return run_serve(args)
     return run_ours(args)
 
 
