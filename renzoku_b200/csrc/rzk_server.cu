@@ -4,12 +4,14 @@
 // request is admitted only if the device memory it will hold while in flight (its receivers
 // and, for a gather, its per-chunk partial sums) fits the server's HBM budget next to the
 // requests already admitted; otherwise the call returns RZK_ERR_BUSY at once and the caller
-// decides whether to retry.  One worker thread owns a context and a stream: each iteration
-// takes the queue, traces every request's primary hits, runs all of the iteration's gathers
-// as ONE persistent batched launch (continuous batching: requests that arrive while a launch
-// runs join the next one), launches guided renders one by one, and marks each request done
-// from a stream host function when its last kernel has finished.  With batching off the
-// worker takes one request at a time and runs it with its own launches (the plain
+// decides whether to retry.  One worker thread owns a context and a stream and keeps at
+// most two launch groups on it (one running, one queued behind it, so the GPU never waits
+// for the host).  Whenever a slot frees it re-orders everything not yet launched - requests
+// waiting over 2 s first, then shortest estimated work first - and issues the next group:
+// consecutive gathers as ONE persistent batched launch of at most ~2e9 evaluations, or one
+// guided render (continuous batching: new requests compete for the very next slot).  A host
+// function after a group's last kernel marks its requests done.  With batching off the
+// worker issues one request at a time in arrival order with its own launches (the plain
 // per-request baseline).  Scratch comes from the stream-ordered allocator, so an iteration
 // neither blocks on an allocation nor synchronises the device.
 #include "rzk_internal.cuh"
@@ -39,8 +41,13 @@ struct Req {
     rzk_status status = RZK_OK;
     double t_submit = 0.0, t_done = 0.0;
     rzk_receiver *d_recv = nullptr;
+    double cost = 0.0;        // estimated work, for ordering an iteration
     struct rzk_server *srv = nullptr;
 };
+
+constexpr double kLaunchCost = 2e9;   // work of one batched launch (~0.1 s of gather)
+constexpr double kAgeMs = 2000.0;     // waiting longer than this overrides shortest-first
+constexpr int kMaxInFlight = 2;       // launch groups on the stream: one running, one queued
 
 int default_chunks(int n_vpl) {   // rzk_gather's automatic chunk count
     const int max_chunks = std::max(1, (n_vpl + 127) / 128);
@@ -60,51 +67,75 @@ struct rzk_server {
     bool stop = false;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
-    std::deque<Req *> queue;
+    std::deque<Req *> queue;     // submitted, not yet seen by the worker
+    std::vector<Req *> ready;    // seen by the worker, not yet launched
+    int in_flight = 0;           // launch groups issued and not finished
     std::unordered_map<uint64_t, Req *> reqs;
     std::thread worker;
 };
 
 namespace {
 
-void CUDART_CB on_done(void *p) {
-    Req *q = (Req *)p;
-    rzk_server *s = q->srv;
-    std::lock_guard<std::mutex> lk(s->mu);
-    q->t_done = now_ms();
-    q->state = q->status == RZK_OK ? kDone : kFailed;
-    s->held -= (int64_t)q->bytes;
-    s->n_completed++;
+// One launch group: the requests whose kernels were issued together; the host function
+// after the group's last kernel marks them done.
+struct Group {
+    rzk_server *s = nullptr;
+    std::vector<Req *> reqs;
+    int64_t launches = 0;
+};
+
+void CUDART_CB on_group_done(void *p) {
+    Group *g = (Group *)p;
+    rzk_server *s = g->s;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        const double t = now_ms();
+        for (Req *q : g->reqs) {
+            q->t_done = t;
+            q->state = q->status == RZK_OK ? kDone : kFailed;
+            s->held -= (int64_t)q->bytes;
+            s->n_completed++;
+        }
+        s->n_launches += g->launches;
+        s->in_flight--;
+    }
     s->cv_done.notify_all();
+    s->cv_work.notify_all();
+    delete g;
 }
 
-void fail_now(rzk_server *s, Req *q, rzk_status st) {
-    std::lock_guard<std::mutex> lk(s->mu);
-    q->status = st;
-    q->t_done = now_ms();
-    q->state = kFailed;
-    s->held -= (int64_t)q->bytes;
-    s->n_completed++;
-    s->cv_done.notify_all();
-}
-
-// the receivers of every request of the iteration, then its gathers (batched or one by
-// one) and its guided renders; each request's completion is a host function on the stream
-void run_iteration(rzk_server *s, std::vector<Req *> &batch) {
+// Issues one group: every request's primary hits, then its gathers as one batched launch
+// (or, without batching, the request's own launches) or its guided render.
+void launch_group(rzk_server *s, Group *g) {
     cudaStream_t st = s->st;
     std::vector<Req *> live;
-    for (Req *q : batch) {
+    for (Req *q : g->reqs) {
         const size_t n = (size_t)q->r.camera.width * q->r.camera.height;
-        cudaError_t e = cudaMallocAsync((void **)&q->d_recv, sizeof(rzk_receiver) * n, st);
-        if (e != cudaSuccess) { fail_now(s, q, RZK_ERR_NOMEM); continue; }
-        rzk_status r = rzk_primary(q->r.scene, &q->r.camera, q->d_recv, st);
-        if (r != RZK_OK) { cudaFreeAsync(q->d_recv, st); fail_now(s, q, r); continue; }
-        live.push_back(q);
+        if (cudaMallocAsync((void **)&q->d_recv, sizeof(rzk_receiver) * n, st) != cudaSuccess) {
+            q->d_recv = nullptr;
+            q->status = RZK_ERR_NOMEM;
+            continue;
+        }
+        q->status = rzk_primary(q->r.scene, &q->r.camera, q->d_recv, st);
+        g->launches++;
+        if (q->status == RZK_OK) live.push_back(q);
     }
-    std::vector<Req *> gathers, guided;
-    for (Req *q : live) (q->r.kind == RZK_REQ_GATHER ? gathers : guided).push_back(q);
-    int64_t launches = 0;
-    if (!gathers.empty() && s->prm.batching) {
+    std::vector<Req *> gathers;
+    for (Req *q : live) {
+        const rzk_request &r = q->r;
+        if (r.kind == RZK_REQ_GUIDED) {
+            rzk_guided_params gp{r.spp, r.max_bounce, r.rr_depth, r.rr_prob, 1, r.seed};
+            q->status = rzk_guided_render(s->ctx, r.scene, r.lightslice, &r.camera, &gp, r.d_rgb, nullptr, st);
+            g->launches++;
+        } else if (!s->prm.batching) {
+            q->status = rzk_gather_cfg(s->ctx, r.scene, q->d_recv, r.camera.width * r.camera.height, r.camera.width,
+                                       r.d_vpls, r.n_vpl, r.clamp_mode, r.tau, r.scale, r.d_rgb, 0, 0, st);
+            g->launches += 3;
+        } else {
+            gathers.push_back(q);
+        }
+    }
+    if (!gathers.empty()) {
         std::vector<rzk_gather_job> jobs(gathers.size());
         for (size_t i = 0; i < gathers.size(); ++i) {
             const rzk_request &r = gathers[i]->r;
@@ -122,55 +153,80 @@ void run_iteration(rzk_server *s, std::vector<Req *> &batch) {
                 r = RZK_ERR_NOMEM;
         }
         if (r == RZK_OK) r = rzk::batch_plan_launch(plan, partial, work, 0, 0, st);
-        if (r == RZK_OK) launches += 1 + 2 * rzk::batch_plan_tables(plan);
+        if (r == RZK_OK) g->launches += 1 + 2 * rzk::batch_plan_tables(plan);
         if (partial) cudaFreeAsync(partial, st);
         if (work) cudaFreeAsync(work, st);
         if (plan) rzk::batch_plan_destroy(plan);
-        for (Req *q : gathers) {
-            q->status = r;
-            cudaFreeAsync(q->d_recv, st);
-            cudaLaunchHostFunc(st, on_done, q);
-        }
-    } else {
-        for (Req *q : gathers) {
-            const rzk_request &r = q->r;
-            q->status = rzk_gather_cfg(s->ctx, r.scene, q->d_recv, r.camera.width * r.camera.height, r.camera.width,
-                                       r.d_vpls, r.n_vpl, r.clamp_mode, r.tau, r.scale, r.d_rgb, 0, 0, st);
-            launches += 3;
-            cudaFreeAsync(q->d_recv, st);
-            cudaLaunchHostFunc(st, on_done, q);
+        for (Req *q : gathers) q->status = r;
+    }
+    for (Req *q : g->reqs)
+        if (q->d_recv) cudaFreeAsync(q->d_recv, st);
+    if (cudaLaunchHostFunc(st, on_group_done, g) != cudaSuccess) {
+        // the stream cannot run host functions: finish the group here
+        cudaStreamSynchronize(st);
+        for (Req *q : g->reqs)
+            if (q->status == RZK_OK) q->status = RZK_ERR_CUDA;
+        on_group_done(g);
+    }
+}
+
+// Picks the next group from the ready list (called with the lock held).  Batching:
+// requests waiting longer than kAgeMs first in arrival order, then shortest estimated work
+// first; consecutive gathers form one group while their total work stays within
+// kLaunchCost; a guided render is a group of its own.  Without batching: arrival order,
+// one request per group.
+Group *next_group(rzk_server *s) {
+    std::vector<Req *> &rd = s->ready;
+    if (rd.empty()) return nullptr;
+    Group *g = new Group();
+    g->s = s;
+    if (!s->prm.batching) {
+        g->reqs.push_back(rd.front());
+        rd.erase(rd.begin());
+        return g;
+    }
+    const double now = now_ms();
+    std::stable_sort(rd.begin(), rd.end(), [now](const Req *a, const Req *b) {
+        const bool aa = now - a->t_submit > kAgeMs, ab = now - b->t_submit > kAgeMs;
+        if (aa != ab) return aa;
+        if (aa) return a->id < b->id;
+        return a->cost < b->cost;
+    });
+    const int max_batch = s->prm.max_batch > 0 ? s->prm.max_batch : 256;
+    size_t take = 1;
+    if (rd.front()->r.kind == RZK_REQ_GATHER) {
+        double cost = rd.front()->cost;
+        while (take < rd.size() && (int)take < max_batch && rd[take]->r.kind == RZK_REQ_GATHER &&
+               cost + rd[take]->cost <= kLaunchCost) {
+            cost += rd[take]->cost;
+            ++take;
         }
     }
-    for (Req *q : guided) {
-        const rzk_request &r = q->r;
-        rzk_guided_params g{r.spp, r.max_bounce, r.rr_depth, r.rr_prob, 1, r.seed};
-        q->status = rzk_guided_render(s->ctx, r.scene, r.lightslice, &r.camera, &g, r.d_rgb, nullptr, st);
-        launches += 1;
-        cudaFreeAsync(q->d_recv, st);
-        cudaLaunchHostFunc(st, on_done, q);
-    }
-    std::lock_guard<std::mutex> lk(s->mu);
-    s->n_launches += launches + (int64_t)live.size();
+    g->reqs.assign(rd.begin(), rd.begin() + take);
+    rd.erase(rd.begin(), rd.begin() + take);
+    return g;
 }
 
 void worker_main(rzk_server *s) {
     cudaSetDevice(s->device);
-    const int max_batch = s->prm.max_batch > 0 ? s->prm.max_batch : 256;
     while (true) {
-        std::vector<Req *> batch;
+        Group *g = nullptr;
         {
             std::unique_lock<std::mutex> lk(s->mu);
-            s->cv_work.wait(lk, [&] { return s->stop || !s->queue.empty(); });
-            if (s->queue.empty()) break;   // stopping and drained
-            const size_t take = s->prm.batching ? std::min<size_t>(s->queue.size(), (size_t)max_batch) : 1;
-            for (size_t i = 0; i < take; ++i) {
-                Req *q = s->queue.front();
+            s->cv_work.wait(lk, [&] {
+                const bool work = !s->queue.empty() || !s->ready.empty();
+                return (s->stop && !work) || (work && s->in_flight < kMaxInFlight);
+            });
+            while (!s->queue.empty()) {
+                s->ready.push_back(s->queue.front());
                 s->queue.pop_front();
-                q->state = kRunning;
-                batch.push_back(q);
             }
+            if (s->ready.empty()) break;   // stopping and drained
+            g = next_group(s);
+            for (Req *q : g->reqs) q->state = kRunning;
+            s->in_flight++;
         }
-        run_iteration(s, batch);
+        launch_group(s, g);
     }
     cudaStreamSynchronize(s->st);
 }
@@ -254,6 +310,7 @@ rzk_status rzk_server_submit(rzk_server *s, const rzk_request *req, uint64_t *ti
     q->bytes = bytes;
     q->srv = s;
     q->t_submit = now_ms();
+    q->cost = r.kind == RZK_REQ_GATHER ? (double)n * (double)std::max(r.n_vpl, 1) : (double)n * r.spp * 32.0;
     s->held += (int64_t)bytes;
     s->reqs[q->id] = q;
     s->queue.push_back(q);
@@ -305,7 +362,10 @@ rzk_status rzk_server_cancel(rzk_server *s, uint64_t ticket) {
     if (it == s->reqs.end()) return RZK_ERR_INVALID;
     Req *q = it->second;
     if (q->state != kQueued) return RZK_ERR_BUSY;
-    s->queue.erase(std::find(s->queue.begin(), s->queue.end(), q));
+    auto qi = std::find(s->queue.begin(), s->queue.end(), q);
+    if (qi != s->queue.end()) s->queue.erase(qi);
+    auto ri = std::find(s->ready.begin(), s->ready.end(), q);
+    if (ri != s->ready.end()) s->ready.erase(ri);
     q->state = kCancelled;
     q->status = RZK_OK;
     q->t_done = now_ms();
