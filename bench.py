@@ -321,10 +321,13 @@ def run_ours(args):
         rays_per_eval = cnt["rays"] / pairs
         # CPU baseline: the reference's own gather on this box's host cores, bounded sample
         threads = os.cpu_count() or 1
-        kind, sample, run = cpu_rate(sc, o, recv_np, vpls_np, tau, scale, 10.0, threads)
-        tc = time.perf_counter()
-        run(sample)
-        cpu_v = sample.shape[0] * N_VPL / (time.perf_counter() - tc)
+        if args.skip_cpu:   # profiling runs: the GPU part only
+            kind, cpu_v, sample = "skipped", None, np.zeros(0, sg.RECEIVER_DTYPE)
+        else:
+            kind, sample, run = cpu_rate(sc, o, recv_np, vpls_np, tau, scale, 10.0, threads)
+            tc = time.perf_counter()
+            run(sample)
+            cpu_v = sample.shape[0] * N_VPL / (time.perf_counter() - tc)
         clocks = clk.summary()
         line = {
             "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": ws, "steps": len(times),
@@ -731,7 +734,14 @@ def main():
     ap.add_argument("--duration", type=float, default=3.0, help="serve: seconds of arrivals per rate")
     ap.add_argument("--budget-gb", type=float, default=4.0, help="serve: HBM admission budget")
     ap.add_argument("--instances", type=int, default=64)
+    ap.add_argument("--vpls", type=int, default=0,
+                    help="scaled: VPL count (default 32,768; smaller for profiling captures)")
+    ap.add_argument("--skip-cpu", action="store_true",
+                    help="scaled: leave out the CPU-baseline leg (profiling runs)")
     args = ap.parse_args()
+    if args.vpls > 0:
+        global N_VPL
+        N_VPL = args.vpls
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "batch":
