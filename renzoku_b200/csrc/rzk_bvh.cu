@@ -563,6 +563,18 @@ rzk_status bvh_build(rzk_scene *s, cudaStream_t st) {
         RZK_CUDA_TRY(cudaGetLastError());
     }
     RZK_CUDA_TRY(cudaStreamSynchronize(st));
+    // the any-hit traversal tree (rzk_sah.cu); without it any-hit walks the reference tree
+    if (s->build_trav) {
+        rzk_status r = build_sah_tree(s, st);
+        if (r == RZK_ERR_STACK) {   // too deep for the traversal stack: walk the reference tree
+            if (s->d_trav) cudaFree(s->d_trav);
+            s->d_trav = nullptr;
+            s->device_bytes -= s->trav_bytes;
+            s->trav_bytes = 0;
+        } else if (r != RZK_OK) {
+            return r;
+        }
+    }
     return RZK_OK;
 }
 

@@ -109,7 +109,7 @@ static void free_scene(rzk_scene *s) {
                     s->d_bmin, s->d_bmax, s->d_codes, s->d_sorted_codes, s->d_perm, s->d_start,
                     s->d_end, s->d_left, s->d_right, s->d_level, s->d_nbmin, s->d_nbmax,
                     s->d_nodes, s->d_tri_isect, s->d_tri_shade, s->d_surf, s->d_mats,
-                    s->d_lights, s->d_light_pdf, s->d_light_cdf, s->d_wide};
+                    s->d_lights, s->d_light_pdf, s->d_light_cdf, s->d_wide, s->d_trav};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     delete s;

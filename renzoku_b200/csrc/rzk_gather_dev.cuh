@@ -148,7 +148,7 @@ __device__ __forceinline__ Rgb pair_radiance(const DevScene &s, const RecvRegs &
 __device__ __forceinline__ bool packet_visible_near(const DevScene &s, const Ray &ray, float tmax, bool act,
                                                     int *stk) {
     if (s.n_nodes == 0) return act;
-    const float4 lo = __ldg(s.nodes + 2), hi = __ldg(s.nodes + 3);
+    const float4 lo = __ldg(s.trav + 2), hi = __ldg(s.trav + 3);
     float t_root = 0.0f;
     bool alive = act && box_hit_fast(lo, hi, ray, s.tmin, tmax, t_root);
     if (!__any_sync(kFull, alive)) return act;
@@ -168,7 +168,7 @@ __device__ __forceinline__ bool packet_visible_near(const DevScene &s, const Ray
     bool overflow = false;
     while (top >= 0) {
         const int c = stk[top--];
-        const float4 *pn = s.nodes + 2 * (c + 1);
+        const float4 *pn = s.trav + 2 * (c + 1);
         const float4 l0 = __ldg(pn), l1 = __ldg(pn + 1), r0 = __ldg(pn + 2), r1 = __ldg(pn + 3);
         const int al = __float_as_int(l0.w), ar = __float_as_int(r0.w);
         float tl = 0.0f, tr = 0.0f;

@@ -43,6 +43,7 @@ struct DevScene {
     const float4 *tri_isect;  // 3 x float4 per sorted triangle (see tri_hit)
     const float4 *tri_shade;  // 2 x float4 per sorted triangle: {n, surf}, {u, -}
     const float4 *wide;       // 8 x float4 per 4-wide traversal node (see rzk_bvh.cu K6)
+    const float4 *trav;       // any-hit tree, same packing as nodes (rzk_sah.cu; = nodes without it)
     const int4 *surf;         // per surface {mat, flags, light, -}
     const rzk_material *mats;
     const DevLight *lights;
@@ -98,6 +99,10 @@ struct rzk_scene {
     float4 *d_nodes = nullptr, *d_tri_isect = nullptr, *d_tri_shade = nullptr;
     float4 *d_wide = nullptr;
     int n_wide = 0, n_wide_cap = 0;
+    float4 *d_trav = nullptr;    // SAH any-hit tree (rzk_sah.cu)
+    int trav_depth = 0;
+    size_t trav_bytes = 0;
+    bool build_trav = true;
     int4 *d_surf = nullptr;
     rzk_material *d_mats = nullptr;
     rzk::DevLight *d_lights = nullptr;
@@ -108,6 +113,7 @@ struct rzk_scene {
     rzk::DevScene dev() const {
         rzk::DevScene s;
         s.nodes = d_nodes; s.tri_isect = d_tri_isect; s.tri_shade = d_tri_shade; s.wide = d_wide;
+        s.trav = d_trav ? d_trav : d_nodes;
         s.surf = d_surf; s.mats = d_mats; s.lights = d_lights; s.light_pdf = d_light_pdf;
         s.light_cdf = d_light_cdf; s.n_tris = n_tris; s.n_nodes = n_nodes; s.n_mats = n_mats;
         s.n_lights = n_lights; s.tmin = tmin; s.err = ctx ? ctx->d_err : nullptr;
@@ -118,6 +124,8 @@ struct rzk_scene {
 namespace rzk {
 // rzk_bvh.cu
 rzk_status bvh_build(rzk_scene *s, cudaStream_t st);
+// rzk_sah.cu
+rzk_status build_sah_tree(rzk_scene *s, cudaStream_t st);
 // utilities (rzk_bvh.cu)
 rzk_status exclusive_scan_i32(const int *d_in, int *d_out, int n, int *d_total, void *d_tmp,
                               size_t tmp_bytes, cudaStream_t st);
