@@ -145,8 +145,12 @@ __device__ __forceinline__ Rgb pair_radiance(const DevScene &s, const RecvRegs &
 
 // Packet any-hit, nearer child first by lane majority.  Returns whether this lane's
 // segment is unoccluded (lanes with act == false return false).
+// `cache` (per lane) names the any-hit-tree leaf whose triangle last occluded this lane's
+// receiver, or -1.  It is tried first: a triangle whose own box and triangle tests pass
+// occludes the segment whichever way it was found, so a hit there is the traversal's
+// answer; the leaf of any triangle the traversal finds replaces it.
 __device__ __forceinline__ bool packet_visible_near(const DevScene &s, const Ray &ray, float tmax, bool act,
-                                                    int *stk) {
+                                                    int *stk, int &cache) {
     if (s.n_nodes == 0) return act;
     const float4 lo = __ldg(s.trav + 2), hi = __ldg(s.trav + 3);
     float t_root = 0.0f;
@@ -161,8 +165,20 @@ __device__ __forceinline__ bool packet_visible_near(const DevScene &s, const Ray
         }
         return act;
     }
-    // lanes whose root test failed cannot reach any triangle below it: they stay visible
     bool occluded = false;
+    if (alive && cache >= 0) {
+        const float4 *pc = s.trav + 2 * (cache + 1);
+        const float4 c0 = __ldg(pc), c1 = __ldg(pc + 1);
+        float tc0 = 0.0f;
+        if (box_hit_fast(c0, c1, ray, s.tmin, tmax, tc0)) {
+            float4 ta, tb, tc;
+            load_tri(s, -1 - __float_as_int(c0.w), ta, tb, tc);
+            if (tri_hit<false>(ta, tb, tc, ray, s.tmin, tmax, nullptr, nullptr, nullptr)) occluded = true;
+        }
+        alive = alive && !occluded;
+        if (!__any_sync(kFull, alive)) return act && !occluded;
+    }
+    // lanes whose root test failed cannot reach any triangle below it: they stay visible
     int top = 0;
     stk[0] = a;
     bool overflow = false;
@@ -174,15 +190,21 @@ __device__ __forceinline__ bool packet_visible_near(const DevScene &s, const Ray
         float tl = 0.0f, tr = 0.0f;
         bool hl = alive && box_hit_fast(l0, l1, ray, s.tmin, tmax, tl);
         bool hr = alive && box_hit_fast(r0, r1, ray, s.tmin, tmax, tr);
-        if (al < 0 && hl) {
+        if (al < 0 && hl && !occluded) {
             float4 ta, tb, tc;
             load_tri(s, -1 - al, ta, tb, tc);
-            if (tri_hit<false>(ta, tb, tc, ray, s.tmin, tmax, nullptr, nullptr, nullptr)) occluded = true;
+            if (tri_hit<false>(ta, tb, tc, ray, s.tmin, tmax, nullptr, nullptr, nullptr)) {
+                occluded = true;
+                cache = c;
+            }
         }
         if (ar < 0 && hr && !occluded) {
             float4 ta, tb, tc;
             load_tri(s, -1 - ar, ta, tb, tc);
-            if (tri_hit<false>(ta, tb, tc, ray, s.tmin, tmax, nullptr, nullptr, nullptr)) occluded = true;
+            if (tri_hit<false>(ta, tb, tc, ray, s.tmin, tmax, nullptr, nullptr, nullptr)) {
+                occluded = true;
+                cache = c + 1;
+            }
         }
         alive = alive && !occluded;
         const bool pl = al >= 0 && __any_sync(kFull, hl && alive);
@@ -261,6 +283,7 @@ __device__ __forceinline__ bool gather_item(const DevScene &s, const rzk_receive
         return true;
     }
     Rgb sum = crgb(0.0f, 0.0f, 0.0f);
+    int occ_cache = -1;   // this lane's last occluder (any-hit tree leaf)
     if (lane == 0) {
         int cnt = min(TILE, j1 - j0);
         fence_proxy_async();
@@ -288,7 +311,7 @@ __device__ __forceinline__ bool gather_item(const DevScene &s, const rzk_receive
             if (!__any_sync(kFull, act)) continue;
             Ray ray = make_ray(r.p, sub(pg.q, r.p));
             float tmax = len(sub(pg.q, r.p)) - s.tmin;
-            if (packet_visible_near(s, ray, tmax, act, ws.stk)) {
+            if (packet_visible_near(s, ray, tmax, act, ws.stk, occ_cache)) {
                 Rgb L = pair_radiance(s, r, rm, l, pg, mode, tau);
                 if (WEIGHTED) {
                     const float w = weights[j0 + k * TILE + v];
