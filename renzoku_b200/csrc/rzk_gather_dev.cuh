@@ -175,9 +175,10 @@ __device__ __forceinline__ bool packet_visible_near(const DevScene &s, const Ray
             load_tri(s, -1 - __float_as_int(c0.w), ta, tb, tc);
             if (tri_hit<false>(ta, tb, tc, ray, s.tmin, tmax, nullptr, nullptr, nullptr)) occluded = true;
         }
-        alive = alive && !occluded;
-        if (!__any_sync(kFull, alive)) return act && !occluded;
     }
+    // every lane takes part in the vote (the cache test above is per lane)
+    alive = alive && !occluded;
+    if (!__any_sync(kFull, alive)) return act && !occluded;
     // lanes whose root test failed cannot reach any triangle below it: they stay visible
     int top = 0;
     stk[0] = a;
