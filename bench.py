@@ -37,6 +37,11 @@ VPL_SEED = 2015
 VPL_PARTICLES = 24000
 MAX_BOUNCE = 3
 TAU_PAIRS = 65536
+# DRAM bytes (read + write) of one full gather launch of this workload, from the one-pass
+# capture `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum -k regex:gather_persistent
+# -s 3 -c 1 python bench.py --steps 1 --warmup 3 --skip-cpu` (41.11 MB read, 69.20 MB
+# written; the writes are the per-chunk partial sums), recorded in profiles/.
+TRAFFIC_BYTES_PER_LAUNCH = (41.11 + 69.20) * 1e6
 
 
 def workload_config():
@@ -339,7 +344,9 @@ def run_ours(args):
                     "h2d_bytes_per_step": n_recv * 96 + N_VPL * 96,
                     "d2h_bytes_per_step": n_recv * 12, "image_finite": img_ok},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak,
+                         "traffic": TRAFFIC_BYTES_PER_LAUNCH if N_VPL == 32768 else None,
+                         "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one full launch",
                          "peak_source": peak_src + " (MEASURED_PEAKS.json hbm_gbs)",
                          "bytes_per_eval": bytes_per_eval,
                          "note": "BVH (~34 MB) and triangles are L2-resident; algorithmic bytes are served mostly from L2"},
