@@ -578,4 +578,50 @@ rzk_status bvh_build(rzk_scene *s, cudaStream_t st) {
     return RZK_OK;
 }
 
+// Stable LSD radix sort of (key, value) pairs on the low `bits` bits of the keys, with the
+// K2 kernels.  keys/vals hold the input; the sorted pairs end in keys/vals (an even number
+// of 8-bit passes) or are copied back there.  scratch: radix_sort_scratch_bytes(n) bytes.
+size_t radix_sort_scratch_bytes(int n) {
+    const int nblocks = (n + kSortTile - 1) / kSortTile;
+    const int hist_n = 256 * std::max(nblocks, 1);
+    auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    return up(sizeof(uint32_t) * (size_t)std::max(n, 1)) + up(sizeof(int) * (size_t)std::max(n, 1)) +
+           2 * up(sizeof(int) * (size_t)hist_n) + up(exclusive_scan_tmp_bytes(hist_n));
+}
+
+rzk_status radix_sort_u32(uint32_t *keys, int *vals, int n, int bits, void *scratch, cudaStream_t st) {
+    if (n <= 1) return RZK_OK;
+    const int nblocks = (n + kSortTile - 1) / kSortTile;
+    const int hist_n = 256 * nblocks;
+    auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    char *p = (char *)scratch;
+    uint32_t *k2 = (uint32_t *)p;
+    p += up(sizeof(uint32_t) * (size_t)n);
+    int *v2 = (int *)p;
+    p += up(sizeof(int) * (size_t)n);
+    int *hist = (int *)p;
+    p += up(sizeof(int) * (size_t)hist_n);
+    int *offs = (int *)p;
+    p += up(sizeof(int) * (size_t)hist_n);
+    void *scan_tmp = p;
+    const size_t scan_bytes = exclusive_scan_tmp_bytes(hist_n);
+    uint32_t *ka = keys, *kb = k2;
+    int *va = vals, *vb = v2;
+    const int passes = std::max(1, (bits + 7) / 8);
+    for (int pass = 0; pass < passes; ++pass) {
+        const int shift = 8 * pass;
+        radix_hist_kernel<<<nblocks, kSortThreads, 0, st>>>(ka, n, shift, hist, nblocks);
+        RZK_TRY(exclusive_scan_i32(hist, offs, hist_n, nullptr, scan_tmp, scan_bytes, st));
+        radix_scatter_kernel<<<nblocks, kSortThreads, 0, st>>>(ka, va, n, shift, offs, nblocks, kb, vb);
+        std::swap(ka, kb);
+        std::swap(va, vb);
+    }
+    RZK_CUDA_TRY(cudaGetLastError());
+    if (ka != keys) {
+        RZK_CUDA_TRY(cudaMemcpyAsync(keys, ka, sizeof(uint32_t) * (size_t)n, cudaMemcpyDeviceToDevice, st));
+        RZK_CUDA_TRY(cudaMemcpyAsync(vals, va, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, st));
+    }
+    return RZK_OK;
+}
+
 }  // namespace rzk

@@ -130,6 +130,8 @@ rzk_status build_sah_tree(rzk_scene *s, cudaStream_t st);
 rzk_status exclusive_scan_i32(const int *d_in, int *d_out, int n, int *d_total, void *d_tmp,
                               size_t tmp_bytes, cudaStream_t st);
 size_t exclusive_scan_tmp_bytes(int n);
+size_t radix_sort_scratch_bytes(int n);
+rzk_status radix_sort_u32(uint32_t *keys, int *vals, int n, int bits, void *scratch, cudaStream_t st);
 // rzk_gather.cu: every (receiver, VPL) pair into a column-major [n_vpl][n_recv][3] matrix;
 // kind 0 radiance, 1 incident radiance, 2 visible x incident radiance (+ visibility)
 rzk_status launch_matrix(const DevScene &s, const rzk_receiver *recv, int n_recv, const rzk_vpl *vpls,

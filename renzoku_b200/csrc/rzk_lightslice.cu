@@ -108,12 +108,33 @@ __global__ void slice_of_kernel(const rzk_receiver *recv, int n, const rzk_mater
     slice[i] = s;
 }
 
-__global__ void bin_pixels_kernel(const int *slice, int n, const int *off, int *cursor, int *pix) {
+__device__ __forceinline__ uint32_t spread_bits(uint32_t v) {   // 16-bit -> even bits
+    v &= 0xffffu;
+    v = (v | (v << 8)) & 0x00ff00ffu;
+    v = (v | (v << 4)) & 0x0f0f0f0fu;
+    v = (v | (v << 2)) & 0x33333333u;
+    v = (v | (v << 1)) & 0x55555555u;
+    return v;
+}
+
+// Sort keys that group the pixels by slice and, within a slice, along a Morton curve of
+// (x, y) when the receivers are an image of width `img_w` (else in pixel order), so that a
+// warp's 32 pixels form a compact patch; pixels without a slice go last.
+__global__ void bin_keys_kernel(const int *slice, int n, int img_w, int mbits, uint32_t *keys, int *vals) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int s = slice[i];
-    if (s < 0) return;
-    pix[off[s] + atomicAdd(cursor + s, 1)] = i;
+    uint32_t k = 0xffffffffu;
+    if (s >= 0) {
+        uint32_t m = 0;
+        if (img_w > 0) {
+            const uint32_t y = (uint32_t)(i / img_w), x = (uint32_t)(i - (int)y * img_w);
+            m = spread_bits(x) | (spread_bits(y) << 1);
+        }
+        k = ((uint32_t)s << mbits) | m;
+    }
+    keys[i] = k;
+    vals[i] = i;
 }
 
 // LightSlice::gather_clusters (lightslice.cc:1315-1345) for the pixels of every slice:
@@ -615,6 +636,8 @@ struct rzk_lightslice {
     DBuf<uint8_t> g_valid;
     // per-gather scratch (grown on demand)
     DBuf<int> d_slice, d_count, d_off, d_cursor, d_pix, d_tile_off, d_work;
+    DBuf<uint32_t> d_keys;
+    DBuf<unsigned char> d_sort;
     DBuf<rzk_receiver> d_perm;
     DBuf<float> d_sums;
 };
@@ -1275,6 +1298,8 @@ rzk_status rzk_lightslice_gather(rzk_lightslice *L, const rzk_receiver *d_recv, 
         LS_TRY(L->d_pix.alloc(n_recv));
         LS_TRY(L->d_perm.alloc(n_recv));
         LS_TRY(L->d_sums.alloc(3 * (size_t)n_recv));
+        LS_TRY(L->d_keys.alloc(n_recv));
+        LS_TRY(L->d_sort.alloc(radix_sort_scratch_bytes(n_recv)));
     }
     if (L->d_count.n < (size_t)ns + 1) {
         LS_TRY(L->d_count.alloc(ns + 1));
@@ -1301,10 +1326,24 @@ rzk_status rzk_lightslice_gather(rzk_lightslice *L, const rzk_receiver *d_recv, 
     const int binned = off[ns];
     LS_TRY(cudaMemcpyAsync(L->d_off.p, off.data(), sizeof(int) * (ns + 1), cudaMemcpyHostToDevice, st));
     LS_TRY(cudaMemcpyAsync(L->d_tile_off.p, toff.data(), sizeof(int) * (ns + 1), cudaMemcpyHostToDevice, st));
-    LS_TRY(cudaMemsetAsync(L->d_cursor.p, 0, sizeof(int) * (ns + 1), st));
-    bin_pixels_kernel<<<(n_recv + 255) / 256, 256, 0, st>>>(L->d_slice.p, n_recv, L->d_off.p, L->d_cursor.p,
-                                                            L->d_pix.p);
+    // bins: a stable sort of the pixels by (slice, Morton code) - see bin_keys_kernel
+    int sbits = 1;
+    while ((1 << sbits) < ns + 1) ++sbits;
+    int img_w = 0, mbits = 0;
+    if (n_recv == L->width * L->height && L->width > 0) {
+        int side = std::max(L->width, L->height), b = 0;
+        while ((1 << b) < side) ++b;
+        if (sbits + 2 * b <= 32) { img_w = L->width; mbits = 2 * b; }
+    }
+    if (sbits + mbits > 32) return RZK_ERR_CAPACITY;
+    bin_keys_kernel<<<(n_recv + 255) / 256, 256, 0, st>>>(L->d_slice.p, n_recv, img_w, mbits, L->d_keys.p,
+                                                          L->d_pix.p);
     LS_TRY(cudaGetLastError());
+    {
+        // pixels without a slice carry all-ones keys: include the slice bits' top value
+        rzk_status rs = radix_sort_u32(L->d_keys.p, L->d_pix.p, n_recv, 32, L->d_sort.p, st);
+        if (rs != RZK_OK) return rs;
+    }
     LS_TRY(cudaMemsetAsync(d_rgb, 0, sizeof(float) * 3 * (size_t)n_recv, st));
     if (binned > 0) {
         gather_recv_kernel<<<(binned + 255) / 256, 256, 0, st>>>(d_recv, L->d_pix.p, binned, L->d_perm.p);
