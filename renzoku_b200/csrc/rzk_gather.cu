@@ -435,7 +435,7 @@ __global__ void __launch_bounds__(kMatBlock) matrix_kernel(DevScene s, const rzk
         if (kind == 2) {
             Ray ray = make_ray(r.p, sub(q, r.p));
             float tmax = len(sub(q, r.p)) - s.tmin;
-            visible = !any_hit<kMatBlock, false>(s, ray, s.tmin, tmax, stk);
+            visible = !any_hit<kMatBlock, false, true>(s, ray, s.tmin, tmax, stk);
             const float vf = visible ? 1.0f : 0.0f;
             L = crgb(vf * L.r, vf * L.g, vf * L.b);
         }
@@ -443,7 +443,7 @@ __global__ void __launch_bounds__(kMatBlock) matrix_kernel(DevScene s, const rzk
         V3 q = ld3(l.p);
         Ray ray = make_ray(r.p, sub(q, r.p));
         float tmax = len(sub(q, r.p)) - s.tmin;
-        if (!any_hit<kMatBlock, false>(s, ray, s.tmin, tmax, stk)) {
+        if (!any_hit<kMatBlock, false, true>(s, ray, s.tmin, tmax, stk)) {
             visible = true;
             rzk_material rm = load_material(s.mats + r.mat);
             L = shade(s, r, rm, l, mode, tau, q);
@@ -476,7 +476,7 @@ __global__ void __launch_bounds__(kMeanBlock) mean_kernel(DevScene s, const rzk_
             V3 q = ld3(l.p);
             Ray ray = make_ray(r.p, sub(q, r.p));
             float tmax = len(sub(q, r.p)) - s.tmin;
-            if (!any_hit<kMeanBlock, false>(s, ray, s.tmin, tmax, stk)) {
+            if (!any_hit<kMeanBlock, false, true>(s, ray, s.tmin, tmax, stk)) {
                 rzk_material rm = load_material(s.mats + r.mat);
                 Rgb L = shade(s, r, rm, l, RZK_CLAMP_NONE, 0.0f, q);
                 val = (double)cval(L);

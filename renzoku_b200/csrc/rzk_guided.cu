@@ -65,7 +65,7 @@ __device__ Rgb first_bounce(const DevScene &s, const GuideRecv &r, const rzk_mat
     if (pdf > 0.0f) {
         Ray sr = make_ray(p, sub(q, p));
         const float tmax = len(sub(q, p)) - s.tmin;
-        if (!any_hit<STRIDE, false>(s, sr, s.tmin, tmax, stk)) {
+        if (!any_hit<STRIDE, false, true>(s, sr, s.tmin, tmax, stk)) {
             const V3 wi = unit(sub(q, p));
             const Rgb Le = light_query(L, q, qn, neg(wi));
             const float G = form_factor_abs(p, pn, q, qn);

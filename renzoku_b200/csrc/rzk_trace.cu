@@ -20,7 +20,7 @@ __global__ void __launch_bounds__(kTraceBlock) occluded_kernel(DevScene s, const
     V3 a = ld3(p + 3 * i), b = ld3(q + 3 * i);
     Ray r = make_ray(a, sub(b, a));
     float tmax = len(sub(b, a)) - s.tmin;
-    out[i] = any_hit<kTraceBlock, false>(s, r, s.tmin, tmax, stk) ? 1 : 0;
+    out[i] = any_hit<kTraceBlock, false, true>(s, r, s.tmin, tmax, stk) ? 1 : 0;
 }
 
 __global__ void __launch_bounds__(kTraceBlock) closest_kernel(DevScene s, const float *o,

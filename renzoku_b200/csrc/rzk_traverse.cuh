@@ -44,11 +44,14 @@ __device__ __forceinline__ void load_tri(const DevScene &s, int slot, float4 &a,
     a = __ldg(p); b = __ldg(p + 1); c = __ldg(p + 2);
 }
 
-template <int STRIDE, bool STATS>
+// TRAV: walk the any-hit tree (DevScene::trav) instead of the reference tree; the answer is
+// the same (see rzk_sah.cu), only the visit order differs.
+template <int STRIDE, bool STATS, bool TRAV = false>
 __device__ __forceinline__ bool any_hit(const DevScene &s, const Ray &r, float tmin, float tmax,
                                         Stack<STRIDE> &stk, TraceStats *ts = nullptr) {
     if (s.n_nodes == 0) return false;
-    float4 lo = __ldg(s.nodes + 2), hi = __ldg(s.nodes + 3);
+    const float4 *tree = TRAV ? s.trav : s.nodes;
+    float4 lo = __ldg(tree + 2), hi = __ldg(tree + 3);
     if (!box_hit(lo, hi, r, tmin, tmax)) return false;
     int a = __float_as_int(lo.w);
     float4 ta, tb, tc;
@@ -63,7 +66,7 @@ __device__ __forceinline__ bool any_hit(const DevScene &s, const Ray &r, float t
     while (!stk.empty()) {
         int c = stk.pop();
         if (STATS) ts->inner++;
-        const float4 *p = s.nodes + 2 * (c + 1);
+        const float4 *p = tree + 2 * (c + 1);
         float4 l0 = __ldg(p), l1 = __ldg(p + 1), r0 = __ldg(p + 2), r1 = __ldg(p + 3);
         bool hl = box_hit(l0, l1, r, tmin, tmax);
         bool hr = box_hit(r0, r1, r, tmin, tmax);
