@@ -189,11 +189,8 @@ __device__ __forceinline__ bool packet_visible_near(const DevScene &s, const Ray
         const float4 l0 = __ldg(pn), l1 = __ldg(pn + 1), r0 = __ldg(pn + 2), r1 = __ldg(pn + 3);
         const int al = __float_as_int(l0.w), ar = __float_as_int(r0.w);
         float tl = 0.0f, tr = 0.0f;
-        // leaves: the exact test; inner nodes of the any-hit tree (flag w = 1): the fused one
-        bool hl = alive && (__float_as_int(l1.w) == 1 ? box_hit_fma(l0, l1, ray, s.tmin, tmax, tl)
-                                                      : box_hit_fast(l0, l1, ray, s.tmin, tmax, tl));
-        bool hr = alive && (__float_as_int(r1.w) == 1 ? box_hit_fma(r0, r1, ray, s.tmin, tmax, tr)
-                                                      : box_hit_fast(r0, r1, ray, s.tmin, tmax, tr));
+        bool hl = alive && box_hit_fast(l0, l1, ray, s.tmin, tmax, tl);
+        bool hr = alive && box_hit_fast(r0, r1, ray, s.tmin, tmax, tr);
         if (al < 0 && hl && !occluded) {
             float4 ta, tb, tc;
             load_tri(s, -1 - al, ta, tb, tc);

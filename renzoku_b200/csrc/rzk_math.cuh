@@ -159,26 +159,6 @@ __device__ __forceinline__ bool box_hit_fast(float4 lo, float4 hi, const Ray &r,
     return tminbox <= tmaxbox;
 }
 
-// Conservative slab test for inner nodes of the any-hit tree, whose boxes are enlarged
-// outward by 2^-16 x the scene's largest coordinate magnitude M: with fused multiply-adds
-// each distance is within one rounding of t (plus one of v * inv_d) of the exact-order
-// value, and for ray origins within 4M that is far less than the enlargement moves it, so
-// the test passes wherever the exact test passes on the unenlarged box.  Leaves are never
-// tested with it.
-__device__ __forceinline__ bool box_hit_fma(float4 lo, float4 hi, const Ray &r, float tmin, float tmax,
-                                            float &tnear) {
-    float x0 = __fmaf_rn(lo.x, r.inv_d.x, r.org_inv_d.x);
-    float y0 = __fmaf_rn(lo.y, r.inv_d.y, r.org_inv_d.y);
-    float z0 = __fmaf_rn(lo.z, r.inv_d.z, r.org_inv_d.z);
-    float x1 = __fmaf_rn(hi.x, r.inv_d.x, r.org_inv_d.x);
-    float y1 = __fmaf_rn(hi.y, r.inv_d.y, r.org_inv_d.y);
-    float z1 = __fmaf_rn(hi.z, r.inv_d.z, r.org_inv_d.z);
-    float tminbox = fmaxf(fmaxf(tmin, fminf(x0, x1)), fmaxf(fminf(y0, y1), fminf(z0, z1)));
-    float tmaxbox = fminf(fminf(tmax, fmaxf(x0, x1)), fminf(fmaxf(y0, y1), fmaxf(z0, z1)));
-    tnear = tminbox;
-    return tminbox <= tmaxbox;
-}
-
 // Triangle::hit (triangle.cc:158-275) on a packed record:
 //   a = {p0.x, p0.y, p0.z, A}, b = {B, C, D, E}, c = {F, -, -, -}
 // with (A,B,C) = p0 - p1 and (D,E,F) = p0 - p2, exactly the reference's p01 / p02.

@@ -13,15 +13,10 @@
 // Built on the host with binned SAH (32 bins on the centroid axis of largest extent; a
 // median split past depth 32 or when the centroids coincide), nodes numbered depth-first
 // with siblings adjacent, packed like the reference tree (two float4 per node slot).
-// Inner boxes are enlarged outward by 2^-16 x the scene's largest coordinate magnitude and
-// flagged (second w = 1) so the packet gathers may test them with fused multiply-adds
-// (box_hit_fma); an enlarged ancestor passes wherever its exact box does, so the argument
-// above still holds.  Leaf boxes stay exact.
 #include "rzk_internal.cuh"
 
 #include <algorithm>
 #include <cfloat>
-#include <cmath>
 #include <cstring>
 #include <vector>
 
@@ -61,15 +56,9 @@ struct Builder {
         std::memcpy(&f, &a, sizeof(f));
         return f;
     }
-    float grow_by = 0.0f;   // outward enlargement of inner boxes (see box_hit_fma)
     void write(int node, const Box &b, int a) {
-        if (a >= 0) {   // inner node: conservative box for the fused slab test
-            out[2 * (node + 1)] = make_float4(b.mn[0] - grow_by, b.mn[1] - grow_by, b.mn[2] - grow_by, bits(a));
-            out[2 * (node + 1) + 1] = make_float4(b.mx[0] + grow_by, b.mx[1] + grow_by, b.mx[2] + grow_by, bits(1));
-        } else {        // leaf: the triangle's exact box
-            out[2 * (node + 1)] = make_float4(b.mn[0], b.mn[1], b.mn[2], bits(a));
-            out[2 * (node + 1) + 1] = make_float4(b.mx[0], b.mx[1], b.mx[2], bits(0));
-        }
+        out[2 * (node + 1)] = make_float4(b.mn[0], b.mn[1], b.mn[2], bits(a));
+        out[2 * (node + 1) + 1] = make_float4(b.mx[0], b.mx[1], b.mx[2], bits(0));
     }
 
     // returns the node's box; the node's record is written here
@@ -171,11 +160,6 @@ rzk_status build_sah_tree(rzk_scene *s, cudaStream_t st) {
         }
     }
     Builder b(box);
-    {
-        float m = 1e-3f;
-        for (int d = 0; d < 6; ++d) m = std::max(m, std::fabs(s->box[d]));
-        b.grow_by = m * (1.0f / 65536.0f);
-    }
     b.cen.resize(3 * (size_t)n);
     for (int slot = 0; slot < n; ++slot)
         for (int d = 0; d < 3; ++d) b.cen[3 * (size_t)slot + d] = 0.5f * (box[slot].mn[d] + box[slot].mx[d]);
