@@ -48,3 +48,18 @@ def test_invalid_arguments_rejected_without_gpu():
     assert lib.rzk_scene_create(None, None, None, None) == rzk.ERR_INVALID
     assert lib.rzk_gather(None, None, None, 0, None, 0, 0, 0.0, 1.0, None, None) == rzk.ERR_INVALID
     assert lib.rzk_camera_setup(None, None, None, 45.0, 1, 1, 1.0, 1.0, None) == rzk.ERR_INVALID
+
+
+def test_new_entry_points_reject_bad_arguments_without_gpu():
+    import ctypes
+    from renzoku_b200 import rzk
+    lib = rzk.load()
+    out = ctypes.c_void_p()
+    bad = rzk.ServerParamsC(-1, 1, 0)
+    assert lib.rzk_server_create(0, ctypes.byref(bad), ctypes.byref(out)) == rzk.ERR_INVALID
+    assert lib.rzk_server_submit(None, None, None) == rzk.ERR_INVALID
+    assert lib.rzk_guided_render(None, None, None, None, None, None, None, None) == rzk.ERR_INVALID
+    assert lib.rzk_lightslice_create(None, None, None, 4, 4, None, 0, None, None, None) == rzk.ERR_INVALID
+    assert lib.rzk_batch_create(None, None, 0, 0, 0, None) == rzk.ERR_INVALID
+    p = rzk.lightslice_params()
+    assert p.num_clusters == 600 and p.max_slice_size == 256 and p.num_neighbor_slices == 16
