@@ -289,26 +289,31 @@ __device__ __forceinline__ float guide_pdf_map(const GuideDev &G, int s, V3 dir)
     return pdf_unit_disk * 0.5f;
 }
 
-// LightSlice::multi_slice_pdf (lightslice.cc:1930-2056) with JENSEN maps
-__device__ __forceinline__ float guide_pdf(const GuideDev &G, const GuideRecv &r, const float *p6, V3 wi) {
+// LightSlice::multi_slice_pdf (lightslice.cc:1930-2056) with JENSEN maps; `s` is
+// guide_slice(G, r, p6) (a function of the receiver alone, so callers compute it once)
+__device__ __forceinline__ float guide_pdf_at(const GuideDev &G, const GuideRecv &r, int s, V3 wi) {
     if (r.mat < 0) return 0.0f;
     if (dot(r.ns, wi) <= 0.0f) return 0.0f;
-    const int s = guide_slice(G, r, p6);
     if (s < 0) return INV_2PI;
     const V3 dir = l2w(guide_rec_onb(G, s), w2l(r.uvn, wi));
     return guide_pdf_map(G, s, dir);
 }
 
+__device__ __forceinline__ float guide_pdf(const GuideDev &G, const GuideRecv &r, const float *p6, V3 wi) {
+    if (r.mat < 0 || dot(r.ns, wi) <= 0.0f) return 0.0f;
+    return guide_pdf_at(G, r, guide_slice(G, r, p6), wi);
+}
+
 // LightSlice::multi_slice_sample (lightslice.cc:1569-1707) with sample_map
-// (lightslice.cc:2313-2348); returns the receiver's BRDF for the drawn direction.
-__device__ __forceinline__ Rgb guide_sample(const GuideDev &G, const GuideRecv &r, const rzk_material &m,
-                                            const float *p6, Rng &g, V3 &wi, float &pdf) {
+// (lightslice.cc:2313-2348); returns the receiver's BRDF for the drawn direction.  `s` is
+// guide_slice(G, r, p6).
+__device__ __forceinline__ Rgb guide_sample_at(const GuideDev &G, const GuideRecv &r, const rzk_material &m,
+                                               int s, Rng &g, V3 &wi, float &pdf) {
     if (r.mat < 0) {
         wi = mk(0.0f, 0.0f, 0.0f);
         pdf = 0.0f;
         return crgb(0.0f, 0.0f, 0.0f);
     }
-    const int s = guide_slice(G, r, p6);
     if (s < 0) {   // no usable record: uniform hemisphere at the receiver
         const float sx = g.uniform(), sy = g.uniform();
         const float phi = TWO_PI * sx;
@@ -345,7 +350,7 @@ __device__ __forceinline__ Rgb guide_sample(const GuideDev &G, const GuideRecv &
         }
     }
     wi = l2w(r.uvn, w2l(rec, ws));   // same local direction at the receiver
-    pdf = guide_pdf(G, r, p6, wi);
+    pdf = guide_pdf_at(G, r, s, wi);
     return brdf_eval(m, r.uvn, r.wo, wi);
 }
 

@@ -137,11 +137,12 @@ __device__ Rgb trace_path(const DevScene &s, const GuideDev &G, const PtParams &
         }
         float p6[6];
         map6(r, m, G.diag, p6);
+        const int slice = guide_slice(G, r, p6);   // the vertex's sampling record, found once
         V3 wi;
         float pdf;
         Rgb brdf;
         if (is_brdf) brdf = brdf_sample(m, r.uvn, r.wo, g, wi, pdf);
-        else brdf = guide_sample(G, r, m, p6, g, wi, pdf);
+        else brdf = guide_sample_at(G, r, m, slice, g, wi, pdf);
         if (!(pdf > 0.0f)) { value = radiance; break; }
         Ray ray = make_ray(r.p, wi);
         HitGeo h;
@@ -149,7 +150,7 @@ __device__ Rgb trace_path(const DevScene &s, const GuideDev &G, const PtParams &
         if (h.light >= 0) { value = radiance; break; }   // no double count of direct light
         float other;
         if (is_brdf) {
-            other = guide_pdf(G, r, p6, wi);
+            other = guide_pdf_at(G, r, slice, wi);
         } else {
             float rho_d = 0.0f, rho_s = 0.0f;
             if (m.type != RZK_BSDF_LAMBERTIAN) rho_terms(m, rho_d, rho_s);
