@@ -1359,7 +1359,13 @@ int ro_cluster_by_sampling(const float *mat, int rows, int cols, int num_cluster
     int *cen = (int *)malloc(sizeof(int) * num_clusters);
     float *w = (float *)malloc(sizeof(float) * num_clusters);
     int count = 0;
-    while (count < num_clusters) {
+    /* the reference's loop never ends when fewer than num_clusters columns can be drawn;
+       cap the target at the drawable count and bound the draws (as the CUDA build does) */
+    int drawable = 0;
+    for (int i = 0; i < cols; ++i) drawable += pa.pdf[i] > 0.0f;
+    const int target = drawable < num_clusters ? drawable : num_clusters;
+    long long draws = 0;
+    while (count < target && draws++ < 100000000LL) {
         int k; float pk;
         dpdf_sample(&pa, rnd(&g), &k, &pk);
         if (pk == 0.0f) continue;

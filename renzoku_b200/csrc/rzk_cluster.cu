@@ -201,7 +201,15 @@ rzk_status cluster_by_sampling(const float *mat, int rows, int cols, int num_clu
     std::vector<int> cen;
     std::vector<float> w;
     std::vector<int> slot(cols, -1);
-    while ((int)cen.size() < num_clusters) {
+    // The reference draws until it holds num_clusters distinct centres, which never ends
+    // when fewer columns than that can be drawn at all (zero alpha); the target is capped
+    // at the drawable count, and a draw budget bounds a pathological distribution.
+    int drawable = 0;
+    for (int i = 0; i < cols; ++i) drawable += pa.pdf[i] > 0.0f;
+    const int target = std::min(num_clusters, drawable);
+    long long draws = 0;
+    const long long max_draws = 100000000LL;
+    while ((int)cen.size() < target && draws++ < max_draws) {
         int k;
         float pk;
         pa.sample(g.next(), k, pk);
@@ -215,6 +223,11 @@ rzk_status cluster_by_sampling(const float *mat, int rows, int cols, int num_clu
         }
     }
     const int count = (int)cen.size();
+    if (count == 0) {   // nothing can be drawn: no cluster, no assignment
+        *h_n = 0;
+        if (h_mags) std::fill(h_mags, h_mags + cols, 0.0f);
+        return RZK_OK;
+    }
     const size_t n3 = 3 * (size_t)rows;
     DevBuf<int> d_cen, d_owner;
     DevBuf<float> d_w, K, kn, nm, D;
