@@ -588,6 +588,17 @@ rzk_status launch_gather(rzk_context *ctx, const DevScene &s, const rzk_receiver
     return RZK_OK;
 }
 
+// Grows the context's scratch (cudaFree / cudaMalloc synchronise with work still using it).
+rzk_status ensure_scratch(rzk_context *ctx, size_t bytes) {
+    if (bytes <= ctx->partial_bytes) return RZK_OK;
+    if (ctx->d_partial) cudaFree(ctx->d_partial);
+    ctx->d_partial = nullptr;
+    ctx->partial_bytes = 0;
+    RZK_CUDA_TRY(cudaMalloc((void **)&ctx->d_partial, bytes));
+    ctx->partial_bytes = bytes;
+    return RZK_OK;
+}
+
 rzk_status launch_matrix(const DevScene &s, const rzk_receiver *recv, int n_recv, const rzk_vpl *vpls,
                          int n_vpl, int mode, float tau, float *mat, uint8_t *vis, int kind,
                          cudaStream_t st) {

@@ -10,8 +10,9 @@
 // vertices deeper than rr_depth, surviving with probability rr_prob and dividing the
 // continuation by it; rr_depth = 0 turns it off.
 //
-// One thread per pixel loops over its samples; sample s of pixel k is path k * spp + s and
-// draws from the counter-based stream (seed, 6, path).  The recursion is unrolled into a
+// One thread per path (sample s of pixel k is path k * spp + s) drawing from the
+// counter-based stream (seed, 6, path); a second kernel sums each pixel's samples in sample
+// order.  The recursion is unrolled into a
 // chain of vertices whose continuation terms are folded back from the deepest vertex, so
 // every sum is formed in the reference's order.
 #include "rzk_guide.cuh"
@@ -176,32 +177,38 @@ __device__ Rgb trace_path(const DevScene &s, const GuideDev &G, const PtParams &
     return value;
 }
 
-__global__ void __launch_bounds__(kPtBlock) guided_kernel(DevScene s, GuideDev G, PtParams P, float *out,
-                                                          float *paths) {
+// one thread per path: sample s of pixel k is path k * spp + s, so neighbouring threads
+// share a pixel (and their first hit)
+__global__ void __launch_bounds__(kPtBlock) guided_kernel(DevScene s, GuideDev G, PtParams P, float *paths) {
     __shared__ int stack_mem[STACK_CAP * kPtBlock];
-    const int k = blockIdx.x * kPtBlock + threadIdx.x;
+    const long long path = (long long)blockIdx.x * kPtBlock + threadIdx.x;
     const int W = P.cam.width, H = P.cam.height;
-    if (k >= W * H) return;
+    if (path >= (long long)W * H * P.spp) return;
     Stack<kPtBlock> stk;
     stk.init(stack_mem + threadIdx.x);
+    const int k = (int)(path / P.spp);
     const int i = k / W, j = k - i * W;
+    Rng g;
+    g.init(P.seed, 6u, (uint32_t)path);
+    Ray ray = camera_ray(P.cam, i, j);
+    HitGeo h;
+    Rgb L = crgb(0.0f, 0.0f, 0.0f);
+    if (trace_closest(s, ray, stk, h)) L = trace_path(s, G, P, to_recv(h, ray), h.light, g, stk);
+    paths[3 * path] = L.r;
+    paths[3 * path + 1] = L.g;
+    paths[3 * path + 2] = L.b;
+}
+
+// the pixel's mean: its samples summed in sample order, divided by spp
+__global__ void guided_mean_kernel(const float *paths, int n_pix, int spp, float *out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n_pix) return;
     Rgb sum = crgb(0.0f, 0.0f, 0.0f);
-    for (int smp = 0; smp < P.spp; ++smp) {
-        const uint32_t path = (uint32_t)k * (uint32_t)P.spp + (uint32_t)smp;
-        Rng g;
-        g.init(P.seed, 6u, path);
-        Ray ray = camera_ray(P.cam, i, j);
-        HitGeo h;
-        Rgb L = crgb(0.0f, 0.0f, 0.0f);
-        if (trace_closest(s, ray, stk, h)) L = trace_path(s, G, P, to_recv(h, ray), h.light, g, stk);
-        if (paths) {
-            paths[3 * (size_t)path] = L.r;
-            paths[3 * (size_t)path + 1] = L.g;
-            paths[3 * (size_t)path + 2] = L.b;
-        }
-        sum = cadd(sum, L);
+    for (int smp = 0; smp < spp; ++smp) {
+        const float *q = paths + 3 * ((size_t)k * spp + smp);
+        sum = cadd(sum, crgb(q[0], q[1], q[2]));
     }
-    const Rgb avg = cdiv(sum, (float)P.spp);
+    const Rgb avg = cdiv(sum, (float)spp);
     out[3 * (size_t)k] = avg.r;
     out[3 * (size_t)k + 1] = avg.g;
     out[3 * (size_t)k + 2] = avg.b;
@@ -234,8 +241,17 @@ rzk_status rzk_guided_render(rzk_context *ctx, rzk_scene *scene, rzk_lightslice 
     P.direct = q.direct_lighting ? 1 : 0;
     P.seed = q.seed;
     const long long n = (long long)cam->width * cam->height;
-    guided_kernel<<<(unsigned)((n + kPtBlock - 1) / kPtBlock), kPtBlock, 0, st>>>(scene->dev(), G, P, d_rgb,
-                                                                                  d_paths);
+    const long long n_paths = n * q.spp;
+    if (n_paths > (1LL << 31)) return RZK_ERR_CAPACITY;
+    float *paths = d_paths;
+    if (!paths) {   // per-path radiance in the context's scratch
+        r = ensure_scratch(ctx, sizeof(float) * 3 * (size_t)n_paths);
+        if (r != RZK_OK) return r;
+        paths = (float *)ctx->d_partial;
+    }
+    guided_kernel<<<(unsigned)((n_paths + kPtBlock - 1) / kPtBlock), kPtBlock, 0, st>>>(scene->dev(), G, P, paths);
+    RZK_CUDA_TRY(cudaGetLastError());
+    guided_mean_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(paths, (int)n, q.spp, d_rgb);
     RZK_CUDA_TRY(cudaGetLastError());
     return RZK_OK;
 }

@@ -137,6 +137,8 @@ rzk_status radix_sort_u32(uint32_t *keys, int *vals, int n, int bits, void *scra
 rzk_status launch_matrix(const DevScene &s, const rzk_receiver *recv, int n_recv, const rzk_vpl *vpls,
                          int n_vpl, int mode, float tau, float *mat, uint8_t *vis, int kind,
                          cudaStream_t st);
+// rzk_gather.cu: make the context's scratch (d_partial) at least `bytes` long
+rzk_status ensure_scratch(rzk_context *ctx, size_t bytes);
 // rzk_batch.cu: plan a batch (validates jobs; no device work), then launch it on a partial
 // buffer of batch_plan_partial_floats floats and batch_plan_tables work counters; grid 0 =
 // the variant's resident grid.
