@@ -58,6 +58,9 @@ rzk_status rzk_scene_destroy(rzk_scene *scene);
 /* Triangle, node and level counts and the device bytes the scene holds. */
 rzk_status rzk_scene_info(const rzk_scene *scene, int *n_tris, int *n_nodes, int *n_levels,
                           size_t *device_bytes);
+/* Aggregate::get_bounding_box (aggregate.cc:28-30): the box the Morton codes are taken
+ * in, box[6] = min xyz, max xyz. */
+rzk_status rzk_scene_bounding_box(const rzk_scene *scene, float *box);
 
 /* Re-runs the LBVH build on the resident triangles (timing / rebuild after edits).
  * Same result as rzk_scene_create. Synchronises `stream`. */
@@ -115,7 +118,9 @@ rzk_status rzk_vpl_generate(rzk_scene *scene, uint32_t seed, int n_particles, in
  * (vpl.cc:214-230).  Receivers with mat < 0 get black.  This is the per-pixel sum of
  * LightTransportMatrix::fill (light_transport_matrix.cc:16-48) without materialising
  * the matrix, and connect_to_vpl's NONE / POWER_SAMPLING accumulation (vpl.cc:496-520)
- * over all VPLs.  The sum is deterministic (fixed VPL-chunk order). */
+ * over all VPLs.  The sum is deterministic: VPLs are grouped into chunks of nearby VPLs
+ * (a stable sort by the Morton code of their positions) and the chunk sums added in chunk
+ * order, so only the float summation order differs from the reference's VPL order. */
 rzk_status rzk_gather(rzk_context *ctx, rzk_scene *scene, const rzk_receiver *d_recv,
                       int n_recv, const rzk_vpl *d_vpls, int n_vpl, int clamp_mode, float tau,
                       float scale, float *d_rgb, void *stream);
@@ -129,8 +134,10 @@ int rzk_gather_variants(void);
  * then takes an 8 x 4 pixel tile, whose shadow rays are more coherent than a 32-pixel
  * row; 0 = 32 consecutive receivers per warp.  `variant` in [0, rzk_gather_variants()),
  * `n_chunks` VPL chunks (0 = automatic).  Layout and variant never change the image;
- * n_chunks changes only the float summation order, and n_chunks = 1 sums in exactly the
- * reference's order. */
+ * n_chunks changes only the float summation order.  n_chunks = 1 sums in exactly the
+ * reference's order; with more chunks each chunk is a run of the VPLs stably sorted by the
+ * Morton code of their positions in the scene box (nearby VPLs trace coherent shadow
+ * rays), and the chunk sums are added in chunk order. */
 rzk_status rzk_gather_cfg(rzk_context *ctx, rzk_scene *scene, const rzk_receiver *d_recv,
                           int n_recv, int image_width, const rzk_vpl *d_vpls, int n_vpl,
                           int clamp_mode, float tau, float scale, float *d_rgb, int variant,
@@ -217,9 +224,10 @@ int rzk_batch_variants(void);
  * renders one scene per process, integrator_scheduler.cc:54-229). */
 rzk_status rzk_batch_create(rzk_context *ctx, const rzk_gather_job *jobs, int n_jobs, int variant,
                             int chunk_len, rzk_batch **out);
-/* Runs every job of the batch: one memset, then per table of up to 128 jobs one persistent
- * launch and one reduction; no allocation and no synchronisation, so it can be captured in
- * a CUDA graph and replayed.
+/* Runs every job of the batch: one memset, then per table of up to 128 jobs the spatial
+ * ordering of its chunked jobs' VPLs (as rzk_gather_cfg orders them, in one sort), one
+ * persistent launch and one reduction; no allocation and no synchronisation, so it can be
+ * captured in a CUDA graph and replayed.
  * Each job's image equals rzk_gather_cfg's for the same chunk length, bit for bit. */
 rzk_status rzk_batch_run(rzk_batch *batch, void *stream);
 rzk_status rzk_batch_destroy(rzk_batch *batch);
@@ -398,7 +406,8 @@ rzk_status rzk_server_create(int device, const rzk_server_params *params, rzk_se
 /* Finishes every admitted request, then releases the server. */
 rzk_status rzk_server_destroy(rzk_server *server);
 /* Admits the request if the device memory it will hold in flight (receivers, and for a
- * gather its per-chunk partial sums) fits the budget next to the admitted ones, else
+ * gather its per-chunk partial sums and its Morton-ordered VPL copy with the sort's
+ * scratch) fits the budget next to the admitted ones, else
  * returns RZK_ERR_BUSY without queueing it.  Thread-safe.  The caller keeps the scene, the
  * VPLs, the LightSlice and d_rgb alive until the request is done. */
 rzk_status rzk_server_submit(rzk_server *server, const rzk_request *request, uint64_t *ticket);
@@ -411,6 +420,7 @@ rzk_status rzk_server_poll(rzk_server *server, uint64_t ticket, int32_t *state, 
 rzk_status rzk_server_wait(rzk_server *server, uint64_t ticket, int32_t timeout_ms, double *latency_ms);
 /* Withdraws a request that is still queued; RZK_ERR_BUSY once it has been launched. */
 rzk_status rzk_server_cancel(rzk_server *server, uint64_t ticket);
+/* Counters since creation; `launches` counts the kernels the server has launched. */
 rzk_status rzk_server_stats(rzk_server *server, int64_t *submitted, int64_t *rejected, int64_t *completed,
                             int64_t *launches, int64_t *held_bytes, int64_t *budget_bytes);
 

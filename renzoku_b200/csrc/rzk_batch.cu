@@ -3,9 +3,9 @@
 //
 // The batch is described once (rzk_batch_create): tables of up to 128 jobs, each with its
 // scene, receivers, VPLs, clamp and output, and one partial-sum buffer for all of them.
-// rzk_batch_run then issues one memset of the work counters and, per table, the persistent
-// kernel and the chunk reduction - no allocation and no host synchronisation, so it can be
-// captured in a CUDA graph and replayed.  Work items are (job, 8 x 4 receiver
+// rzk_batch_run then issues one memset of the work counters and, per table, the ordering
+// of its chunked jobs' VPLs, the persistent kernel and the chunk reduction - no allocation
+// and no host synchronisation, so it can be captured in a CUDA graph and replayed.  Work items are (job, 8 x 4 receiver
 // tile, VPL chunk), numbered job-major; every warp takes the next item from one atomic
 // counter, so small and large jobs share the SMs without a per-launch tail.  Each job's
 // image is bit-identical to rzk_gather_cfg with the same chunk length.
@@ -119,11 +119,22 @@ int grid_for(int variant) {
 
 // A batch split into launch tables: consecutive jobs go into one launch until it holds
 // kJobsPerLaunch jobs or 2^30 work items.
+// Jobs with several VPL chunks gather from a Morton-ordered copy of their VPLs, exactly as
+// rzk_gather_cfg does: per table one ordering pass writes the copies into the plan's
+// ordering buffer (laid out [sorted VPLs of every table | sort scratch]).
 struct BatchPlan {
     std::vector<JobTable> tables;
+    std::vector<OrderTable> orders;          // per table: the ordered jobs' VPL sets
+    std::vector<std::vector<int>> ordered;   // per table: job slot of each order segment
+    std::vector<size_t> order_base;          // per table: its first VPL in the sorted copy
+    size_t sorted_vpls = 0;
+    int max_order_total = 0;
     size_t partial_floats = 0;
-    float *bound = nullptr;   // partial buffer the tables point into
+    float *bound = nullptr;        // partial buffer the tables point into
+    void *order_bound = nullptr;   // ordering buffer the ordered jobs point into
 };
+
+static size_t up256(size_t b) { return (b + 255) & ~(size_t)255; }
 
 rzk_status batch_plan_create(const rzk_gather_job *jobs, int n_jobs, int chunk_len, BatchPlan **out) {
     if (!jobs || n_jobs <= 0 || !out || chunk_len < 0 || (chunk_len % 128) != 0) return RZK_ERR_INVALID;
@@ -176,6 +187,9 @@ rzk_status batch_plan_create(const rzk_gather_job *jobs, int n_jobs, int chunk_l
             p->tables.emplace_back();
             JobTable &t = p->tables.back();
             memset(&t, 0, sizeof(t));
+            p->orders.emplace_back();
+            order_table_init(p->orders.back());
+            p->ordered.emplace_back();
         }
         JobTable &t = p->tables.back();
         BatchJob &b = h[i];
@@ -183,7 +197,16 @@ rzk_status batch_plan_create(const rzk_gather_job *jobs, int n_jobs, int chunk_l
         b.out_begin = t.n_out;
         t.n_items += (int)items;
         t.n_out += 3LL * b.n_recv;
+        if (b.n_chunks > 1) {   // kJobsPerLaunch == kOrderSegs: the table has room
+            order_table_add(p->orders.back(), b.vpls, b.n_vpl, jobs[i].scene->box);
+            p->ordered.back().push_back(t.n_jobs);
+        }
         t.jobs[t.n_jobs++] = b;
+    }
+    for (const OrderTable &o : p->orders) {
+        p->order_base.push_back(p->sorted_vpls);
+        p->sorted_vpls += (size_t)o.total;
+        p->max_order_total = std::max(p->max_order_total, o.total);
     }
     *out = p;
     return RZK_OK;
@@ -191,23 +214,41 @@ rzk_status batch_plan_create(const rzk_gather_job *jobs, int n_jobs, int chunk_l
 
 void batch_plan_destroy(BatchPlan *p) { delete p; }
 size_t batch_plan_partial_floats(const BatchPlan *p) { return p->partial_floats; }
+size_t batch_plan_order_bytes(const BatchPlan *p) {
+    if (p->sorted_vpls == 0) return 0;
+    return up256(sizeof(rzk_vpl) * p->sorted_vpls) + order_scratch_bytes(p->max_order_total);
+}
 int batch_plan_tables(const BatchPlan *p) { return (int)p->tables.size(); }
+int batch_plan_launches(const BatchPlan *p) {
+    int n = 0;
+    for (const OrderTable &o : p->orders) n += 2 + order_launches(o);
+    return n;
+}
 
-rzk_status batch_plan_launch(BatchPlan *p, float *partial, int *work, int variant, int grid, cudaStream_t st) {
-    if (p->bound != partial) {
+rzk_status batch_plan_launch(BatchPlan *p, float *partial, void *order, int *work, int variant, int grid,
+                             cudaStream_t st) {
+    if (p->sorted_vpls > 0 && (!order || ((uintptr_t)order & 15u))) return RZK_ERR_INVALID;
+    rzk_vpl *sorted = (rzk_vpl *)order;
+    if (p->bound != partial || p->order_bound != order) {
         size_t off = 0;
         for (JobTable &t : p->tables)
             for (int i = 0; i < t.n_jobs; ++i) {
                 t.jobs[i].partial = partial + off;
                 off += 3ull * t.jobs[i].n_recv * t.jobs[i].n_chunks;
             }
+        for (size_t k = 0; k < p->tables.size(); ++k)
+            for (int g = 0; g < p->orders[k].n_segs; ++g)
+                p->tables[k].jobs[p->ordered[k][g]].vpls = sorted + p->order_base[k] + p->orders[k].seg[g].begin;
         p->bound = partial;
+        p->order_bound = order;
     }
     if (grid <= 0) grid = grid_for(variant);
+    void *scratch = p->sorted_vpls > 0 ? (char *)order + up256(sizeof(rzk_vpl) * p->sorted_vpls) : nullptr;
     RZK_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(int) * p->tables.size(), st));
     for (size_t k = 0; k < p->tables.size(); ++k) {
         const JobTable &t = p->tables[k];
         int *w = work + k;
+        if (p->orders[k].total > 0) RZK_TRY(order_vpls(p->orders[k], scratch, sorted + p->order_base[k], st));
         switch (variant) {
             case 0: batch_gather_kernel<4, 32, 5><<<grid, 128, 0, st>>>(t, w); break;
             case 1: batch_gather_kernel<4, 32, 4><<<grid, 128, 0, st>>>(t, w); break;
@@ -227,6 +268,7 @@ struct rzk_batch {
     rzk_context *ctx = nullptr;
     rzk::BatchPlan *plan = nullptr;
     float *d_partial = nullptr;
+    void *d_order = nullptr;             // Morton-ordered VPL copies and sort scratch
     int *d_work = nullptr;               // one work counter per table
     int n_jobs = 0, variant = 0, grid = 0;
 };
@@ -240,6 +282,7 @@ int rzk_batch_variants(void) { return (int)(sizeof(kBatchVariants) / sizeof(kBat
 rzk_status rzk_batch_destroy(rzk_batch *b) {
     if (!b) return RZK_ERR_INVALID;
     if (b->d_partial) cudaFree(b->d_partial);
+    if (b->d_order) cudaFree(b->d_order);
     if (b->d_work) cudaFree(b->d_work);
     if (b->plan) batch_plan_destroy(b->plan);
     delete b;
@@ -267,6 +310,8 @@ rzk_status rzk_batch_create(rzk_context *ctx, const rzk_gather_job *jobs, int n_
     cudaError_t e = cudaMalloc((void **)&bt->d_partial, sizeof(float) * std::max<size_t>(plan->partial_floats, 1));
     if (e != cudaSuccess) return fail(e);
     if ((e = cudaMalloc((void **)&bt->d_work, sizeof(int) * plan->tables.size())) != cudaSuccess) return fail(e);
+    const size_t ob = batch_plan_order_bytes(plan);
+    if (ob > 0 && (e = cudaMalloc(&bt->d_order, ob)) != cudaSuccess) return fail(e);
     bt->grid = grid_for(variant);
     *out = bt;
     return RZK_OK;
@@ -274,7 +319,8 @@ rzk_status rzk_batch_create(rzk_context *ctx, const rzk_gather_job *jobs, int n_
 
 rzk_status rzk_batch_run(rzk_batch *b, void *stream) {
     if (!b) return RZK_ERR_INVALID;
-    return batch_plan_launch(b->plan, b->d_partial, b->d_work, b->variant, b->grid, (cudaStream_t)stream);
+    return batch_plan_launch(b->plan, b->d_partial, b->d_order, b->d_work, b->variant, b->grid,
+                             (cudaStream_t)stream);
 }
 
 rzk_status rzk_batch_autotune(rzk_context *ctx, const rzk_gather_job *jobs, int n_jobs, int max_probe_jobs,

@@ -411,7 +411,6 @@ rzk_status dalloc(T **p, size_t count, size_t *acc) {
 
 }  // namespace
 
-#define RZK_TRY(expr) do { rzk_status _s = (expr); if (_s != RZK_OK) return _s; } while (0)
 
 rzk_status bvh_build(rzk_scene *s, cudaStream_t st) {
     const int n = s->n_tris;
@@ -587,6 +586,20 @@ size_t radix_sort_scratch_bytes(int n) {
     auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
     return up(sizeof(uint32_t) * (size_t)std::max(n, 1)) + up(sizeof(int) * (size_t)std::max(n, 1)) +
            2 * up(sizeof(int) * (size_t)hist_n) + up(exclusive_scan_tmp_bytes(hist_n));
+}
+
+int exclusive_scan_launches(int n, bool total) {
+    if (n <= 0) return 0;
+    const int nb = (n + kScanItems - 1) / kScanItems;
+    const int k = nb == 1 ? 1 : 2 + exclusive_scan_launches(nb, false);
+    return k + (total ? 1 : 0);
+}
+
+int radix_sort_launches(int n, int bits) {
+    if (n <= 1) return 0;
+    const int nblocks = (n + kSortTile - 1) / kSortTile;
+    const int passes = std::max(1, (bits + 7) / 8);
+    return passes * (2 + exclusive_scan_launches(256 * nblocks, false));
 }
 
 rzk_status radix_sort_u32(uint32_t *keys, int *vals, int n, int bits, void *scratch, cudaStream_t st) {

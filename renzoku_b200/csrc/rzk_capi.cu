@@ -22,9 +22,9 @@ rzk_status launch_occluded(const DevScene &s, const float *p, const float *q, in
 rzk_status launch_closest(const DevScene &s, const float *o, const float *d, int n, float *t,
                           rzk_receiver *recv, cudaStream_t st);
 rzk_status launch_primary(const DevScene &s, const rzk_camera &cam, rzk_receiver *out, cudaStream_t st);
-rzk_status launch_gather(rzk_context *ctx, const DevScene &s, const rzk_receiver *recv, int n_recv,
-                         int img_w, const rzk_vpl *vpls, int n_vpl, int mode, float tau, float scale,
-                         float *out, int variant, int n_chunks, cudaStream_t st);
+rzk_status launch_gather(rzk_context *ctx, const DevScene &s, const float *box, const rzk_receiver *recv,
+                         int n_recv, int img_w, const rzk_vpl *vpls, int n_vpl, int mode, float tau,
+                         float scale, float *out, int variant, int n_chunks, cudaStream_t st);
 int gather_variant_count();
 rzk_status launch_mean(rzk_context *ctx, const DevScene &s, const rzk_receiver *recv, int n_recv,
                        const rzk_vpl *vpls, int n_vpl, uint32_t seed, int n_pairs, double *h_mean,
@@ -39,7 +39,6 @@ rzk_status launch_vplgen(rzk_scene *sc, uint32_t seed, int n_particles, int max_
 
 using namespace rzk;
 
-#define RZK_TRY(expr) do { rzk_status _s = (expr); if (_s != RZK_OK) return _s; } while (0)
 
 static inline cudaStream_t as_stream(void *s) { return (cudaStream_t)s; }
 static inline bool aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
@@ -88,6 +87,7 @@ rzk_status rzk_context_destroy(rzk_context *c) {
     if (c->d_partial) cudaFree(c->d_partial);
     if (c->d_stage) cudaFree(c->d_stage);
     if (c->d_work) cudaFree(c->d_work);
+    if (c->d_order) cudaFree(c->d_order);
     delete c;
     return RZK_OK;
 }
@@ -208,6 +208,12 @@ rzk_status rzk_scene_info(const rzk_scene *s, int *n_tris, int *n_nodes, int *n_
     return RZK_OK;
 }
 
+rzk_status rzk_scene_bounding_box(const rzk_scene *s, float *box) {
+    if (!s || !box) return RZK_ERR_INVALID;
+    for (int i = 0; i < 6; ++i) box[i] = s->box[i];
+    return RZK_OK;
+}
+
 rzk_status rzk_scene_rebuild(rzk_scene *s, void *stream) {
     if (!s) return RZK_ERR_INVALID;
     return bvh_build(s, as_stream(stream));
@@ -321,8 +327,8 @@ rzk_status rzk_gather_cfg(rzk_context *ctx, rzk_scene *s, const rzk_receiver *d_
                           float scale, float *d_rgb, int variant, int n_chunks, void *stream) {
     RZK_TRY(check_gather_args(ctx, s, d_recv, n_recv, d_vpls, n_vpl, clamp_mode));
     if ((n_recv > 0 && !d_rgb) || image_width < 0) return RZK_ERR_INVALID;
-    return launch_gather(ctx, s->dev(), d_recv, n_recv, image_width, d_vpls, n_vpl, clamp_mode, tau, scale,
-                         d_rgb, variant, n_chunks, as_stream(stream));
+    return launch_gather(ctx, s->dev(), s->box, d_recv, n_recv, image_width, d_vpls, n_vpl, clamp_mode, tau,
+                         scale, d_rgb, variant, n_chunks, as_stream(stream));
 }
 
 rzk_status rzk_gather(rzk_context *ctx, rzk_scene *s, const rzk_receiver *d_recv, int n_recv,
@@ -355,8 +361,8 @@ rzk_status rzk_gather_host(rzk_context *ctx, rzk_scene *s, const rzk_receiver *h
     float *d_out = (float *)((char *)d_vpls + ((vb + 255) & ~(size_t)255));
     if (rb) RZK_CUDA_TRY(cudaMemcpyAsync(d_recv, h_recv, rb, cudaMemcpyHostToDevice, st));
     if (vb) RZK_CUDA_TRY(cudaMemcpyAsync(d_vpls, h_vpls, vb, cudaMemcpyHostToDevice, st));
-    RZK_TRY(launch_gather(ctx, s->dev(), d_recv, n_recv, image_width, d_vpls, n_vpl, clamp_mode, tau, scale,
-                          d_out, 0, 0, st));
+    RZK_TRY(launch_gather(ctx, s->dev(), s->box, d_recv, n_recv, image_width, d_vpls, n_vpl, clamp_mode, tau,
+                          scale, d_out, 0, 0, st));
     if (ob) RZK_CUDA_TRY(cudaMemcpyAsync(h_rgb, d_out, ob, cudaMemcpyDeviceToHost, st));
     RZK_CUDA_TRY(cudaStreamSynchronize(st));
     return RZK_OK;

@@ -3,7 +3,8 @@
 // (VirtualPointLight::gather_point, vpl.cc:661-688), summed per shading point.
 //
 // Layout: a CTA owns BLOCK consecutive receivers (one per thread, loaded once into
-// registers) and one contiguous chunk of VPLs.  The chunk streams through shared memory
+// registers) and one contiguous chunk of VPLs (with several chunks, of the VPLs sorted by
+// the Morton code of their positions).  The chunk streams through shared memory
 // in TILE-VPL tiles, double-buffered, each tile one bulk copy (cp.async.bulk, no
 // multicast) completing on an mbarrier.  Every thread walks the tile in VPL order; the
 // shading term is evaluated first and the shadow ray is traced only when it is non-zero
@@ -499,7 +500,136 @@ __global__ void mean_final_kernel(const double *block_sums, int nb, int n_pairs,
     *out = n_pairs > 0 ? acc / n_pairs : 0.0;
 }
 
+// 8 bits spread to every third bit (bit i -> bit 3i).
+__device__ __forceinline__ uint32_t spread3(uint32_t x) {
+    x &= 0xffu;
+    x = (x | (x << 16)) & 0x030000ffu;
+    x = (x | (x << 8)) & 0x0300f00fu;
+    x = (x | (x << 4)) & 0x030c30c3u;
+    x = (x | (x << 2)) & 0x09249249u;
+    return x;
+}
+
+// segment holding concatenated position i (segments in order of begin)
+__device__ __forceinline__ int order_seg_of(const OrderTable &t, int i) {
+    int lo = 0, hi = t.n_segs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (t.seg[mid].begin <= i) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Key of concatenated VPL i: its segment in the top bits, below them the 24-bit Morton
+// code of its position on a 256^3 grid over the segment's box (positions outside the box
+// clamp to the border cells, NaN to cell 0).
+__global__ void order_keys_kernel(const __grid_constant__ OrderTable t, uint32_t *keys, int *idx) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= t.total) return;
+    const int sg = order_seg_of(t, i);
+    const OrderSeg &g = t.seg[sg];
+    const rzk_vpl &v = g.src[i - g.begin];
+    auto cell = [](float x) { return (uint32_t)fminf(fmaxf(x, 0.0f), 255.0f); };
+    const uint32_t x = cell((v.p[0] - g.lo[0]) * g.k[0]);
+    const uint32_t y = cell((v.p[1] - g.lo[1]) * g.k[1]);
+    const uint32_t z = cell((v.p[2] - g.lo[2]) * g.k[2]);
+    keys[i] = ((uint32_t)sg << 24) | (spread3(x) << 2) | (spread3(y) << 1) | spread3(z);
+    idx[i] = i;
+}
+
+// out[j] = concatenated VPL idx[j], one 4-byte word per thread (coalesced writes; each
+// record's 96 bytes are read by 24 consecutive threads).
+__global__ void order_permute_kernel(const __grid_constant__ OrderTable t, const int *idx, rzk_vpl *out) {
+    constexpr int W = (int)(sizeof(rzk_vpl) / 4);
+    const long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= (long long)t.total * W) return;
+    const int j = (int)(w / W), c = (int)(w % W);
+    const int i = idx[j];
+    const OrderSeg &g = t.seg[order_seg_of(t, i)];
+    reinterpret_cast<uint32_t *>(out)[w] = reinterpret_cast<const uint32_t *>(g.src + (i - g.begin))[c];
+}
+
 }  // namespace
+
+// Spatial order of a chunked gather's VPLs.  With several chunks the image is a sum of
+// per-chunk sums anyway, so which VPLs share a chunk changes only the float summation
+// order; chunks of nearby VPLs make the consecutive shadow rays of a warp end near one
+// another, so they walk the same tree nodes (L1 hits) and the per-lane occluder cache hits
+// more often.  One stable radix sort orders all segments of a table at once (segment in
+// the top key bits, ties keep push order).
+static_assert(sizeof(OrderTable) <= 32000, "kernel parameter block limit");
+
+void order_table_init(OrderTable &t) {
+    t.n_segs = 0;
+    t.total = 0;
+}
+
+bool order_table_add(OrderTable &t, const rzk_vpl *src, int n, const float *box) {
+    if (t.n_segs == kOrderSegs) return false;
+    OrderSeg &g = t.seg[t.n_segs++];
+    g.src = src;
+    g.begin = t.total;
+    g.n = n;
+    for (int d = 0; d < 3; ++d) {
+        const float ext = box[3 + d] - box[d];
+        g.lo[d] = box[d];
+        g.k[d] = ext > 0.0f ? 256.0f / ext : 0.0f;
+    }
+    t.total += n;
+    return true;
+}
+
+static int order_bits(const OrderTable &t) {
+    int b = 0;
+    while ((1 << b) < t.n_segs) ++b;
+    return 24 + b;
+}
+
+static size_t order_up(size_t b) { return (b + 255) & ~(size_t)255; }
+
+size_t order_scratch_bytes(int total) {
+    return 2 * order_up(sizeof(uint32_t) * (size_t)total) + radix_sort_scratch_bytes(total);
+}
+
+int order_launches(const OrderTable &t) {
+    return t.total > 0 ? 2 + radix_sort_launches(t.total, order_bits(t)) : 0;
+}
+
+rzk_status order_vpls(const OrderTable &t, void *scratch, rzk_vpl *out, cudaStream_t st) {
+    if (t.total <= 0) return RZK_OK;
+    char *p = (char *)scratch;
+    uint32_t *keys = (uint32_t *)p;
+    int *idx = (int *)(p + order_up(sizeof(uint32_t) * (size_t)t.total));
+    void *sort = p + 2 * order_up(sizeof(uint32_t) * (size_t)t.total);
+    order_keys_kernel<<<(t.total + 255) / 256, 256, 0, st>>>(t, keys, idx);
+    RZK_CUDA_TRY(cudaGetLastError());
+    RZK_TRY(radix_sort_u32(keys, idx, t.total, order_bits(t), sort, st));
+    const long long words = (long long)t.total * (long long)(sizeof(rzk_vpl) / 4);
+    order_permute_kernel<<<(unsigned)((words + 255) / 256), 256, 0, st>>>(t, idx, out);
+    RZK_CUDA_TRY(cudaGetLastError());
+    return RZK_OK;
+}
+
+// Orders one gather's VPLs into the context's buffer: [sorted VPLs | sort scratch].
+static rzk_status order_gather_vpls(rzk_context *ctx, const float *box, const rzk_vpl *vpls, int n_vpl,
+                                    const rzk_vpl **sorted, cudaStream_t st) {
+    const size_t vb = order_up(sizeof(rzk_vpl) * (size_t)n_vpl);
+    const size_t need = vb + order_scratch_bytes(n_vpl);
+    if (need > ctx->order_bytes) {
+        if (ctx->d_order) cudaFree(ctx->d_order);
+        ctx->d_order = nullptr;
+        ctx->order_bytes = 0;
+        RZK_CUDA_TRY(cudaMalloc(&ctx->d_order, need));
+        ctx->order_bytes = need;
+    }
+    OrderTable t;
+    order_table_init(t);
+    order_table_add(t, vpls, n_vpl, box);
+    rzk_vpl *out = (rzk_vpl *)ctx->d_order;
+    RZK_TRY(order_vpls(t, (char *)ctx->d_order + vb, out, st));
+    *sorted = out;
+    return RZK_OK;
+}
 
 // Tile configurations compiled in; the autotuner picks one per workload.
 //   kind 3: persistent warp-packet kernel (the production path)      variants 0-3
@@ -529,9 +659,37 @@ static int persistent_grid(rzk_context *ctx, int variant) {
     return ctx->persistent_grid[variant];
 }
 
-rzk_status launch_gather(rzk_context *ctx, const DevScene &s, const rzk_receiver *recv, int n_recv,
-                         int img_w, const rzk_vpl *vpls, int n_vpl, int mode, float tau, float scale,
-                         float *out, int variant, int n_chunks, cudaStream_t st) {
+// Chunk count and length of a gather (n_chunks <= 0: automatic).  Chunk boundaries are
+// multiples of 128 VPLs whatever the variant's tile, so every variant sums the same VPLs in
+// the same order for a given n_chunks.
+static void resolve_chunks(int n_vpl, int &n_chunks, int &chunk_len) {
+    const int max_chunks = std::max(1, (n_vpl + 127) / 128);
+    if (n_chunks <= 0) n_chunks = std::min(32, max_chunks);   // ~1k-VPL chunks at 32k VPLs
+    n_chunks = std::min(std::min(n_chunks, max_chunks), 65535);
+    if (n_vpl <= 0) n_chunks = 1;
+    chunk_len = n_vpl > 0 ? (n_vpl + n_chunks - 1) / n_chunks : 0;
+    chunk_len = (chunk_len + 127) / 128 * 128;
+    if (chunk_len > 0) n_chunks = (n_vpl + chunk_len - 1) / chunk_len;
+}
+
+int gather_launches(int n_recv, int n_vpl, int n_chunks) {
+    if (n_recv <= 0) return 0;
+    int chunk_len = 0;
+    resolve_chunks(n_vpl, n_chunks, chunk_len);
+    int k = 2;   // gather + chunk reduction
+    if (n_chunks > 1) {
+        OrderTable t;
+        order_table_init(t);
+        const float box[6] = {0, 0, 0, 1, 1, 1};
+        order_table_add(t, nullptr, n_vpl, box);
+        k += order_launches(t);
+    }
+    return k;
+}
+
+rzk_status launch_gather(rzk_context *ctx, const DevScene &s, const float *box, const rzk_receiver *recv,
+                         int n_recv, int img_w, const rzk_vpl *vpls, int n_vpl, int mode, float tau,
+                         float scale, float *out, int variant, int n_chunks, cudaStream_t st) {
     if (n_recv <= 0) return RZK_OK;
     if (variant < 0 || variant >= gather_variant_count()) variant = 0;
     const GatherVariant gv = kVariants[variant];
@@ -543,15 +701,8 @@ rzk_status launch_gather(rzk_context *ctx, const DevScene &s, const rzk_receiver
     } else {
         wtiles = ((long long)n_recv + 31) / 32;
     }
-    const int max_chunks = std::max(1, (n_vpl + 127) / 128);
-    if (n_chunks <= 0) n_chunks = std::min(32, max_chunks);   // ~1k-VPL chunks at 32k VPLs
-    n_chunks = std::min(std::min(n_chunks, max_chunks), 65535);
-    if (n_vpl <= 0) n_chunks = 1;
-    // chunk boundaries are multiples of 128 VPLs whatever the variant's tile, so every
-    // variant sums the same VPLs in the same order for a given n_chunks
-    int chunk_len = n_vpl > 0 ? (n_vpl + n_chunks - 1) / n_chunks : 0;
-    chunk_len = (chunk_len + 127) / 128 * 128;
-    if (chunk_len > 0) n_chunks = (n_vpl + chunk_len - 1) / chunk_len;
+    int chunk_len = 0;
+    resolve_chunks(n_vpl, n_chunks, chunk_len);
     size_t need = sizeof(float) * 3 * (size_t)n_recv * n_chunks;
     if (need > ctx->partial_bytes) {
         if (ctx->d_partial) cudaFree(ctx->d_partial);
@@ -562,6 +713,7 @@ rzk_status launch_gather(rzk_context *ctx, const DevScene &s, const rzk_receiver
     }
     if (!ctx->d_work) RZK_CUDA_TRY(cudaMalloc((void **)&ctx->d_work, 64));
     float *part = ctx->d_partial;
+    if (n_chunks > 1) RZK_TRY(order_gather_vpls(ctx, box, vpls, n_vpl, &vpls, st));
     if (gv.kind == 3) {
         RZK_CUDA_TRY(cudaMemsetAsync(ctx->d_work, 0, sizeof(int), st));
         const int wt = (int)wtiles;

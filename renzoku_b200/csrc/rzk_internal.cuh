@@ -16,6 +16,7 @@
             return _e == cudaErrorMemoryAllocation ? RZK_ERR_NOMEM : RZK_ERR_CUDA; \
         }                                                    \
     } while (0)
+#define RZK_TRY(expr) do { rzk_status _s = (expr); if (_s != RZK_OK) return _s; } while (0)
 
 namespace rzk {
 
@@ -72,6 +73,9 @@ struct rzk_context {
     double *d_mean = nullptr;
     // work counter of the persistent gather and its resident grid size per variant
     int *d_work = nullptr;
+    // Morton-ordered VPL copy of a chunked gather, its sort keys and sort scratch
+    void *d_order = nullptr;
+    size_t order_bytes = 0;
     int persistent_grid[16] = {0};
 };
 
@@ -132,19 +136,47 @@ rzk_status exclusive_scan_i32(const int *d_in, int *d_out, int n, int *d_total, 
 size_t exclusive_scan_tmp_bytes(int n);
 size_t radix_sort_scratch_bytes(int n);
 rzk_status radix_sort_u32(uint32_t *keys, int *vals, int n, int bits, void *scratch, cudaStream_t st);
+int exclusive_scan_launches(int n, bool total);   // kernels one exclusive_scan_i32 call launches
+int radix_sort_launches(int n, int bits);         // kernels one radix_sort_u32 call launches
+
+// rzk_gather.cu: spatial VPL order of chunked gathers.  Each segment is one gather's VPL
+// set; ordering writes every segment's VPLs, stably sorted by the 24-bit Morton code of
+// their positions on a 256^3 grid over that gather's scene box, to out[begin, begin + n).
+constexpr int kOrderSegs = 128;
+struct OrderSeg {
+    const rzk_vpl *src;
+    int begin, n;
+    float lo[3], k[3];
+};
+struct OrderTable {
+    OrderSeg seg[kOrderSegs];
+    int n_segs, total;
+};
+void order_table_init(OrderTable &t);
+// appends a segment (no device work); false when the table is full
+bool order_table_add(OrderTable &t, const rzk_vpl *src, int n, const float *box);
+size_t order_scratch_bytes(int total);
+int order_launches(const OrderTable &t);
+rzk_status order_vpls(const OrderTable &t, void *scratch, rzk_vpl *out, cudaStream_t st);
 // rzk_gather.cu: every (receiver, VPL) pair into a column-major [n_vpl][n_recv][3] matrix;
 // kind 0 radiance, 1 incident radiance, 2 visible x incident radiance (+ visibility)
 rzk_status launch_matrix(const DevScene &s, const rzk_receiver *recv, int n_recv, const rzk_vpl *vpls,
                          int n_vpl, int mode, float tau, float *mat, uint8_t *vis, int kind,
                          cudaStream_t st);
+// rzk_gather.cu: kernels one rzk_gather_cfg call launches
+int gather_launches(int n_recv, int n_vpl, int n_chunks);
 // rzk_gather.cu: make the context's scratch (d_partial) at least `bytes` long
 rzk_status ensure_scratch(rzk_context *ctx, size_t bytes);
 // rzk_batch.cu: plan a batch (validates jobs; no device work), then launch it on a partial
-// buffer of batch_plan_partial_floats floats and batch_plan_tables work counters; grid 0 =
-// the variant's resident grid.
+// buffer of batch_plan_partial_floats floats, an ordering buffer of batch_plan_order_bytes
+// bytes (16-byte aligned; null when that is 0) and batch_plan_tables work counters;
+// grid 0 = the variant's resident grid.
 rzk_status batch_plan_create(const rzk_gather_job *jobs, int n_jobs, int chunk_len, BatchPlan **out);
 void batch_plan_destroy(BatchPlan *p);
 size_t batch_plan_partial_floats(const BatchPlan *p);
+size_t batch_plan_order_bytes(const BatchPlan *p);
 int batch_plan_tables(const BatchPlan *p);
-rzk_status batch_plan_launch(BatchPlan *p, float *partial, int *work, int variant, int grid, cudaStream_t st);
+int batch_plan_launches(const BatchPlan *p);   // kernels one batch_plan_launch launches
+rzk_status batch_plan_launch(BatchPlan *p, float *partial, void *order, int *work, int variant, int grid,
+                             cudaStream_t st);
 }  // namespace rzk

@@ -126,11 +126,11 @@ void launch_group(rzk_server *s, Group *g) {
         if (r.kind == RZK_REQ_GUIDED) {
             rzk_guided_params gp{r.spp, r.max_bounce, r.rr_depth, r.rr_prob, 1, r.seed};
             q->status = rzk_guided_render(s->ctx, r.scene, r.lightslice, &r.camera, &gp, r.d_rgb, nullptr, st);
-            g->launches++;
+            g->launches += 2;   // path kernel + per-pixel mean
         } else if (!s->prm.batching) {
             q->status = rzk_gather_cfg(s->ctx, r.scene, q->d_recv, r.camera.width * r.camera.height, r.camera.width,
                                        r.d_vpls, r.n_vpl, r.clamp_mode, r.tau, r.scale, r.d_rgb, 0, 0, st);
-            g->launches += 3;
+            g->launches += rzk::gather_launches(r.camera.width * r.camera.height, r.n_vpl, 0);
         } else {
             gathers.push_back(q);
         }
@@ -145,16 +145,19 @@ void launch_group(rzk_server *s, Group *g) {
         rzk::BatchPlan *plan = nullptr;
         rzk_status r = rzk::batch_plan_create(jobs.data(), (int)jobs.size(), 0, &plan);
         float *partial = nullptr;
+        void *order = nullptr;
         int *work = nullptr;
         if (r == RZK_OK) {
-            const size_t pf = rzk::batch_plan_partial_floats(plan);
+            const size_t pf = rzk::batch_plan_partial_floats(plan), ob = rzk::batch_plan_order_bytes(plan);
             if (cudaMallocAsync((void **)&partial, sizeof(float) * std::max<size_t>(pf, 1), st) != cudaSuccess ||
+                (ob > 0 && cudaMallocAsync(&order, ob, st) != cudaSuccess) ||
                 cudaMallocAsync((void **)&work, sizeof(int) * rzk::batch_plan_tables(plan), st) != cudaSuccess)
                 r = RZK_ERR_NOMEM;
         }
-        if (r == RZK_OK) r = rzk::batch_plan_launch(plan, partial, work, 0, 0, st);
-        if (r == RZK_OK) g->launches += 1 + 2 * rzk::batch_plan_tables(plan);
+        if (r == RZK_OK) r = rzk::batch_plan_launch(plan, partial, order, work, 0, 0, st);
+        if (r == RZK_OK) g->launches += rzk::batch_plan_launches(plan);
         if (partial) cudaFreeAsync(partial, st);
+        if (order) cudaFreeAsync(order, st);
         if (work) cudaFreeAsync(work, st);
         if (plan) rzk::batch_plan_destroy(plan);
         for (Req *q : gathers) q->status = r;
@@ -290,6 +293,8 @@ rzk_status rzk_server_submit(rzk_server *s, const rzk_request *req, uint64_t *ti
             r.clamp_mode < RZK_CLAMP_NONE || r.clamp_mode > RZK_CLAMP_RADIANCE)
             return RZK_ERR_INVALID;
         bytes += sizeof(float) * 3 * (size_t)n * (size_t)default_chunks(r.n_vpl);
+        if (default_chunks(r.n_vpl) > 1)   // Morton-ordered VPL copy and its sort scratch
+            bytes += sizeof(rzk_vpl) * (size_t)r.n_vpl + rzk::order_scratch_bytes(r.n_vpl);
     } else if (r.kind == RZK_REQ_GUIDED) {
         if (!r.lightslice || r.spp <= 0 || r.max_bounce < 1 || r.max_bounce > 16 || r.rr_depth < 0 ||
             (r.rr_depth > 0 && !(r.rr_prob > 0.0f && r.rr_prob <= 1.0f)))

@@ -45,6 +45,7 @@ SIGNATURES = [
     ("rzk_scene_create", I32, [P, P, P, P]),
     ("rzk_scene_destroy", I32, [P]),
     ("rzk_scene_info", I32, [P, P, P, P, P]),
+    ("rzk_scene_bounding_box", I32, [P, P]),
     ("rzk_scene_rebuild", I32, [P, P]),
     ("rzk_bvh_dump", I32, [P, P, P, P, I32, P]),
     ("rzk_morton_codes", I32, [P, P, P]),
@@ -240,6 +241,12 @@ class AggregateCuda:
         check(self.lib.rzk_bvh_dump(self.h, codes.ctypes.data, perm.ctypes.data, nodes.ctypes.data,
                                     self.n_nodes, _stream_ptr()), "rzk_bvh_dump")
         return codes, perm, nodes
+
+    def bounding_box(self) -> np.ndarray:
+        """Aggregate::get_bounding_box: float32 [6] = min xyz, max xyz."""
+        box = np.zeros(6, np.float32)
+        check(self.lib.rzk_scene_bounding_box(self.h, box.ctypes.data), "rzk_scene_bounding_box")
+        return box
 
     def morton_codes(self):
         codes = np.zeros(self.n_tris, np.uint32)

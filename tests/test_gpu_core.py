@@ -263,7 +263,8 @@ def test_gather_full_scale_variants_agree_and_match_oracle(ctx, oracle_built):
     """The bench workload (512 x 512 receivers, 32,768 VPLs, ~300k triangles): every gather
     variant gives the same image for a fixed chunk count - the warp-packet kernels agree
     bit for bit with the per-thread kernel, whose traversal is the reference's any-hit -
-    and sampled pixels match the oracle summed with the same chunking."""
+    and sampled pixels match the oracle summed with the same chunking (runs of 1,024 of
+    the Morton-ordered VPLs, each summed in order, the runs added in order)."""
     from oracle import Oracle
     from renzoku_b200 import rzk
     sc = sg.room_objects(2000, 512, 512)
@@ -286,6 +287,7 @@ def test_gather_full_scale_variants_agree_and_match_oracle(ctx, oracle_built):
         assert len(bad) == 0, (v, bad[:10])
     recv = rzk.records_from_device(recv_t, sg.RECEIVER_DTYPE)
     vpls = rzk.records_from_device(vt, sg.VPL_DTYPE)
+    vpls = vpls[morton_order(vpls, agg.bounding_box())].copy()
     rng = np.random.default_rng(7)
     pick = np.sort(rng.choice(np.nonzero(recv["mat"] >= 0)[0], 48, replace=False))
     o = Oracle(sc)
@@ -296,3 +298,47 @@ def test_gather_full_scale_variants_agree_and_match_oracle(ctx, oracle_built):
         acc = part if acc is None else acc + part
     acc = acc * np.float32(1e-4)
     assert np.array_equal(ref[pick], acc)
+
+
+def _spread3(x):
+    x = x.astype(np.uint32) & np.uint32(0xFF)
+    x = (x | (x << 16)) & np.uint32(0x030000FF)
+    x = (x | (x << 8)) & np.uint32(0x0300F00F)
+    x = (x | (x << 4)) & np.uint32(0x030C30C3)
+    x = (x | (x << 2)) & np.uint32(0x09249249)
+    return x
+
+
+def morton_order(vpls, box):
+    """The chunked gather's VPL order, restated: stable by the 24-bit Morton code of the
+    position on a 256^3 grid over the scene box, in float32 as the device forms it."""
+    box = np.asarray(box, np.float32)
+    lo, ext = box[:3], box[3:] - box[:3]
+    k = np.where(ext > 0, np.float32(256.0) / np.where(ext > 0, ext, np.float32(1)), 0).astype(np.float32)
+    c = (vpls["p"].astype(np.float32) - lo) * k
+    c = np.clip(np.nan_to_num(c, nan=0.0), 0.0, 255.0).astype(np.uint32)
+    key = (_spread3(c[:, 0]) << 2) | (_spread3(c[:, 1]) << 1) | _spread3(c[:, 2])
+    return np.argsort(key, kind="stable")
+
+
+def test_chunked_gather_sums_morton_ordered_chunks(big):
+    """With several chunks the gather sums runs of the Morton-ordered VPLs: pre-sorting the
+    VPLs on the host by the same key leaves the image bit-identical, whatever the variant."""
+    from renzoku_b200 import rzk
+    sc, agg, o = big
+    cam = rzk.Camera(sc.camera)
+    recv_t = agg.primary(cam)
+    vpls = o.vpl_generate(29, 700, 4)
+    order = morton_order(vpls, agg.bounding_box())
+    assert not np.array_equal(order, np.arange(len(vpls)))
+    dv, ds = rzk.records_to_device(vpls), rzk.records_to_device(vpls[order].copy())
+    ev = rzk.VirtualPointLightCuda(agg, rzk.CLAMP_RADIANCE, 0.05)
+    n = cam.n_pixels
+    for k in (2, 7):
+        for variant in (0, agg.lib.rzk_gather_variants() - 1):
+            a = ev.gather(recv_t, n, dv, len(vpls), scale=1.0 / 700, image_width=sc.camera.width,
+                          variant=variant, n_chunks=k).cpu().numpy()
+            b = ev.gather(recv_t, n, ds, len(vpls), scale=1.0 / 700, image_width=sc.camera.width,
+                          variant=variant, n_chunks=k).cpu().numpy()
+            assert np.array_equal(a, b), (k, variant, np.abs(a - b).max())
+    agg.ctx.check()
