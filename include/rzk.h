@@ -119,7 +119,7 @@ rzk_status rzk_vpl_generate(rzk_scene *scene, uint32_t seed, int n_particles, in
  * LightTransportMatrix::fill (light_transport_matrix.cc:16-48) without materialising
  * the matrix, and connect_to_vpl's NONE / POWER_SAMPLING accumulation (vpl.cc:496-520)
  * over all VPLs.  The sum is deterministic: VPLs are grouped into chunks of nearby VPLs
- * (a stable sort by the Morton code of their positions) and the chunk sums added in chunk
+ * (a stable sort along a Hilbert curve through their positions) and the chunk sums added in chunk
  * order, so only the float summation order differs from the reference's VPL order. */
 rzk_status rzk_gather(rzk_context *ctx, rzk_scene *scene, const rzk_receiver *d_recv,
                       int n_recv, const rzk_vpl *d_vpls, int n_vpl, int clamp_mode, float tau,
@@ -136,8 +136,8 @@ int rzk_gather_variants(void);
  * `n_chunks` VPL chunks (0 = automatic).  Layout and variant never change the image;
  * n_chunks changes only the float summation order.  n_chunks = 1 sums in exactly the
  * reference's order; with more chunks each chunk is a run of the VPLs stably sorted by the
- * Morton code of their positions in the scene box (nearby VPLs trace coherent shadow
- * rays), and the chunk sums are added in chunk order. */
+ * Hilbert-curve index of their positions' cells on a 256^3 grid over the scene box
+ * (nearby VPLs trace coherent shadow rays), and the chunk sums are added in chunk order. */
 rzk_status rzk_gather_cfg(rzk_context *ctx, rzk_scene *scene, const rzk_receiver *d_recv,
                           int n_recv, int image_width, const rzk_vpl *d_vpls, int n_vpl,
                           int clamp_mode, float tau, float scale, float *d_rgb, int variant,
@@ -406,7 +406,7 @@ rzk_status rzk_server_create(int device, const rzk_server_params *params, rzk_se
 /* Finishes every admitted request, then releases the server. */
 rzk_status rzk_server_destroy(rzk_server *server);
 /* Admits the request if the device memory it will hold in flight (receivers, and for a
- * gather its per-chunk partial sums and its Morton-ordered VPL copy with the sort's
+ * gather its per-chunk partial sums and its spatially ordered VPL copy with the sort's
  * scratch) fits the budget next to the admitted ones, else
  * returns RZK_ERR_BUSY without queueing it.  Thread-safe.  The caller keeps the scene, the
  * VPLs, the LightSlice and d_rgb alive until the request is done. */

@@ -72,8 +72,8 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) batch_gather_kernel(const __
         const int j = find_job(t, item, false);
         const BatchJob &jb = t.jobs[j];
         const int local = item - (int)jb.item_begin;
-        const int chunk = local / jb.n_wtiles;
-        const int wt = local - chunk * jb.n_wtiles;
+        const int wt = local / jb.n_chunks;   // tile-major, as gather_persistent_kernel
+        const int chunk = local - wt * jb.n_chunks;
         if (!gather_item<TILE>(jb.s, jb.recv, jb.n_recv, jb.img_w, jb.vpls, jb.n_vpl, chunk, wt, jb.chunk_len,
                                jb.mode, jb.tau, jb.partial, ws, lane))
             break;
@@ -119,7 +119,7 @@ int grid_for(int variant) {
 
 // A batch split into launch tables: consecutive jobs go into one launch until it holds
 // kJobsPerLaunch jobs or 2^30 work items.
-// Jobs with several VPL chunks gather from a Morton-ordered copy of their VPLs, exactly as
+// Jobs with several VPL chunks gather from a spatially ordered copy of their VPLs, exactly as
 // rzk_gather_cfg does: per table one ordering pass writes the copies into the plan's
 // ordering buffer (laid out [sorted VPLs of every table | sort scratch]).
 struct BatchPlan {
@@ -268,7 +268,7 @@ struct rzk_batch {
     rzk_context *ctx = nullptr;
     rzk::BatchPlan *plan = nullptr;
     float *d_partial = nullptr;
-    void *d_order = nullptr;             // Morton-ordered VPL copies and sort scratch
+    void *d_order = nullptr;             // spatially ordered VPL copies and sort scratch
     int *d_work = nullptr;               // one work counter per table
     int n_jobs = 0, variant = 0, grid = 0;
 };

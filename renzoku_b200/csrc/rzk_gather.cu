@@ -3,8 +3,8 @@
 // (VirtualPointLight::gather_point, vpl.cc:661-688), summed per shading point.
 //
 // Layout: a CTA owns BLOCK consecutive receivers (one per thread, loaded once into
-// registers) and one contiguous chunk of VPLs (with several chunks, of the VPLs sorted by
-// the Morton code of their positions).  The chunk streams through shared memory
+// registers) and one contiguous chunk of VPLs (with several chunks, of the VPLs sorted
+// along a Hilbert curve through their positions).  The chunk streams through shared memory
 // in TILE-VPL tiles, double-buffered, each tile one bulk copy (cp.async.bulk, no
 // multicast) completing on an mbarrier.  Every thread walks the tile in VPL order; the
 // shading term is evaluated first and the shadow ray is traced only when it is non-zero
@@ -383,8 +383,10 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) gather_persistent_kernel(
         if (lane == 0) item = atomicAdd(work, 1);
         item = __shfl_sync(kFull, item, 0);
         if (item >= n_items) break;
-        const int chunk = item / n_wtiles;
-        const int wt = item - chunk * n_wtiles;
+        // tile-major: the warps in flight work on a few hundred neighbouring tiles (a compact
+        // band of ray origins) against every chunk
+        const int wt = item / n_chunks;
+        const int chunk = item - wt * n_chunks;
         if (!gather_item<TILE>(s, recv, n_recv, img_w, vpls, n_vpl, chunk, wt, chunk_len, mode, tau, partial,
                                ws, lane))
             break;
@@ -520,8 +522,38 @@ __device__ __forceinline__ int order_seg_of(const OrderTable &t, int i) {
     return lo;
 }
 
-// Key of concatenated VPL i: its segment in the top bits, below them the 24-bit Morton
-// code of its position on a 256^3 grid over the segment's box (positions outside the box
+// 24-bit index of cell (x, y, z) of a 256^3 grid along a 3-D Hilbert curve: J. Skilling's
+// transform of the axes to the curve's transposed index ("Programming the Hilbert curve",
+// AIP Conf. Proc. 707, 2004) - undo the excess work level by level, then Gray-encode -
+// followed by interleaving the transposed words, first axis most significant.
+__device__ __forceinline__ uint32_t hilbert3_8(uint32_t x, uint32_t y, uint32_t z) {
+    uint32_t a[3] = {x, y, z};
+    for (uint32_t q = 128u; q > 1u; q >>= 1) {
+        const uint32_t p = q - 1u;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            if (a[d] & q) {
+                a[0] ^= p;
+            } else {
+                const uint32_t s = (a[0] ^ a[d]) & p;
+                a[0] ^= s;
+                a[d] ^= s;
+            }
+        }
+    }
+    a[1] ^= a[0];
+    a[2] ^= a[1];
+    uint32_t flip = 0;
+    for (uint32_t q = 128u; q > 1u; q >>= 1)
+        if (a[2] & q) flip ^= q - 1u;
+    a[0] ^= flip;
+    a[1] ^= flip;
+    a[2] ^= flip;
+    return (spread3(a[0]) << 2) | (spread3(a[1]) << 1) | spread3(a[2]);
+}
+
+// Key of concatenated VPL i: its segment in the top bits, below them the Hilbert index of
+// its position's cell on a 256^3 grid over the segment's box (positions outside the box
 // clamp to the border cells, NaN to cell 0).
 __global__ void order_keys_kernel(const __grid_constant__ OrderTable t, uint32_t *keys, int *idx) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -533,7 +565,7 @@ __global__ void order_keys_kernel(const __grid_constant__ OrderTable t, uint32_t
     const uint32_t x = cell((v.p[0] - g.lo[0]) * g.k[0]);
     const uint32_t y = cell((v.p[1] - g.lo[1]) * g.k[1]);
     const uint32_t z = cell((v.p[2] - g.lo[2]) * g.k[2]);
-    keys[i] = ((uint32_t)sg << 24) | (spread3(x) << 2) | (spread3(y) << 1) | spread3(z);
+    keys[i] = ((uint32_t)sg << 24) | hilbert3_8(x, y, z);
     idx[i] = i;
 }
 

@@ -73,7 +73,7 @@ struct rzk_context {
     double *d_mean = nullptr;
     // work counter of the persistent gather and its resident grid size per variant
     int *d_work = nullptr;
-    // Morton-ordered VPL copy of a chunked gather, its sort keys and sort scratch
+    // spatially ordered VPL copy of a chunked gather, its sort keys and sort scratch
     void *d_order = nullptr;
     size_t order_bytes = 0;
     int persistent_grid[16] = {0};
@@ -140,8 +140,9 @@ int exclusive_scan_launches(int n, bool total);   // kernels one exclusive_scan_
 int radix_sort_launches(int n, int bits);         // kernels one radix_sort_u32 call launches
 
 // rzk_gather.cu: spatial VPL order of chunked gathers.  Each segment is one gather's VPL
-// set; ordering writes every segment's VPLs, stably sorted by the 24-bit Morton code of
-// their positions on a 256^3 grid over that gather's scene box, to out[begin, begin + n).
+// set; ordering writes every segment's VPLs, stably sorted by the Hilbert-curve index of
+// their positions' cells on a 256^3 grid over that gather's scene box, to
+// out[begin, begin + n).
 constexpr int kOrderSegs = 128;
 struct OrderSeg {
     const rzk_vpl *src;

@@ -293,7 +293,7 @@ rzk_status rzk_server_submit(rzk_server *s, const rzk_request *req, uint64_t *ti
             r.clamp_mode < RZK_CLAMP_NONE || r.clamp_mode > RZK_CLAMP_RADIANCE)
             return RZK_ERR_INVALID;
         bytes += sizeof(float) * 3 * (size_t)n * (size_t)default_chunks(r.n_vpl);
-        if (default_chunks(r.n_vpl) > 1)   // Morton-ordered VPL copy and its sort scratch
+        if (default_chunks(r.n_vpl) > 1)   // spatially ordered VPL copy and its sort scratch
             bytes += sizeof(rzk_vpl) * (size_t)r.n_vpl + rzk::order_scratch_bytes(r.n_vpl);
     } else if (r.kind == RZK_REQ_GUIDED) {
         if (!r.lightslice || r.spp <= 0 || r.max_bounce < 1 || r.max_bounce > 16 || r.rr_depth < 0 ||

@@ -264,7 +264,7 @@ def test_gather_full_scale_variants_agree_and_match_oracle(ctx, oracle_built):
     variant gives the same image for a fixed chunk count - the warp-packet kernels agree
     bit for bit with the per-thread kernel, whose traversal is the reference's any-hit -
     and sampled pixels match the oracle summed with the same chunking (runs of 1,024 of
-    the Morton-ordered VPLs, each summed in order, the runs added in order)."""
+    the Hilbert-ordered VPLs, each summed in order, the runs added in order)."""
     from oracle import Oracle
     from renzoku_b200 import rzk
     sc = sg.room_objects(2000, 512, 512)
@@ -287,7 +287,7 @@ def test_gather_full_scale_variants_agree_and_match_oracle(ctx, oracle_built):
         assert len(bad) == 0, (v, bad[:10])
     recv = rzk.records_from_device(recv_t, sg.RECEIVER_DTYPE)
     vpls = rzk.records_from_device(vt, sg.VPL_DTYPE)
-    vpls = vpls[morton_order(vpls, agg.bounding_box())].copy()
+    vpls = vpls[spatial_order(vpls, agg.bounding_box())].copy()
     rng = np.random.default_rng(7)
     pick = np.sort(rng.choice(np.nonzero(recv["mat"] >= 0)[0], 48, replace=False))
     o = Oracle(sc)
@@ -309,27 +309,52 @@ def _spread3(x):
     return x
 
 
-def morton_order(vpls, box):
-    """The chunked gather's VPL order, restated: stable by the 24-bit Morton code of the
-    position on a 256^3 grid over the scene box, in float32 as the device forms it."""
+def hilbert3(x, y, z, bits=8):
+    """Index along a 3-D Hilbert curve of cells (x, y, z) of a 2^bits grid: Skilling's
+    axes-to-transpose transform (AIP Conf. Proc. 707, 2004), then the transposed words
+    interleaved, first axis most significant (uint32 arrays)."""
+    a = [np.asarray(v, np.uint32).copy() for v in (x, y, z)]
+    q = np.uint32(1 << (bits - 1))
+    while q > 1:
+        p = np.uint32(q - 1)
+        for d in range(3):
+            hi = (a[d] & q) != 0
+            a[0] = np.where(hi, a[0] ^ p, a[0])
+            s = np.where(hi, np.uint32(0), (a[0] ^ a[d]) & p).astype(np.uint32)
+            a[0] = a[0] ^ s
+            a[d] = a[d] ^ s
+        q = np.uint32(q >> 1)
+    a[1] ^= a[0]
+    a[2] ^= a[1]
+    flip = np.zeros_like(a[2])
+    q = np.uint32(1 << (bits - 1))
+    while q > 1:
+        flip = np.where((a[2] & q) != 0, flip ^ np.uint32(q - 1), flip).astype(np.uint32)
+        q = np.uint32(q >> 1)
+    a = [v ^ flip for v in a]
+    return (_spread3(a[0]) << 2) | (_spread3(a[1]) << 1) | _spread3(a[2])
+
+
+def spatial_order(vpls, box):
+    """The chunked gather's VPL order, restated: stable by the Hilbert index of the
+    position's cell on a 256^3 grid over the scene box, in float32 as the device forms it."""
     box = np.asarray(box, np.float32)
     lo, ext = box[:3], box[3:] - box[:3]
     k = np.where(ext > 0, np.float32(256.0) / np.where(ext > 0, ext, np.float32(1)), 0).astype(np.float32)
     c = (vpls["p"].astype(np.float32) - lo) * k
     c = np.clip(np.nan_to_num(c, nan=0.0), 0.0, 255.0).astype(np.uint32)
-    key = (_spread3(c[:, 0]) << 2) | (_spread3(c[:, 1]) << 1) | _spread3(c[:, 2])
-    return np.argsort(key, kind="stable")
+    return np.argsort(hilbert3(c[:, 0], c[:, 1], c[:, 2]), kind="stable")
 
 
-def test_chunked_gather_sums_morton_ordered_chunks(big):
-    """With several chunks the gather sums runs of the Morton-ordered VPLs: pre-sorting the
+def test_chunked_gather_sums_spatially_ordered_chunks(big):
+    """With several chunks the gather sums runs of the Hilbert-ordered VPLs: pre-sorting the
     VPLs on the host by the same key leaves the image bit-identical, whatever the variant."""
     from renzoku_b200 import rzk
     sc, agg, o = big
     cam = rzk.Camera(sc.camera)
     recv_t = agg.primary(cam)
     vpls = o.vpl_generate(29, 700, 4)
-    order = morton_order(vpls, agg.bounding_box())
+    order = spatial_order(vpls, agg.bounding_box())
     assert not np.array_equal(order, np.arange(len(vpls)))
     dv, ds = rzk.records_to_device(vpls), rzk.records_to_device(vpls[order].copy())
     ev = rzk.VirtualPointLightCuda(agg, rzk.CLAMP_RADIANCE, 0.05)
