@@ -503,6 +503,80 @@ def run_batch(args):
     return 0
 
 
+def run_mrcs(args):
+    """Matrix row-column sampling on the scaled scene: 512 x 512 shading points, the first
+    32,768 VPLs resampled by power to 10,000 columns, 256 stratified rows (32 x 32 strata),
+    327 clusters (1% of the VPLs).  Reports the set-up stages and the gather over the
+    clusters' representatives (every pixel x every representative, one shadow ray each),
+    timed on the device with the L2 flushed between steps.  Prints one JSON line."""
+    import torch
+    from renzoku_b200 import build as rbuild
+    rbuild.build()
+    from renzoku_b200 import rzk, scenegen as sg
+    ctx = rzk.Context(0)
+    sc = sg.room_objects(2000, WIDTH, HEIGHT)
+    agg = rzk.AggregateCuda(ctx, sc)
+    cam = rzk.Camera(sc.camera)
+    recv = agg.primary(cam)
+    vt, n_made = rzk.VplGeneratorCuda(agg).spawn(VPL_SEED, VPL_PARTICLES, MAX_BOUNCE)
+    vt = vt[: N_VPL * 96].contiguous()
+    vpls_np = rzk.records_from_device(vt, sg.VPL_DTYPE)
+    _, num_emitted = select_vpls(vpls_np)
+    ev = rzk.VirtualPointLightCuda(agg, rzk.CLAMP_RADIANCE, 1.0)
+    tau = float(np.float32(0.1 * ev.mean_contribution(recv, cam.n_pixels, vt, N_VPL, seed=VPL_SEED,
+                                                       n_pairs=TAU_PAIRS)))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    m = rzk.MrcsCuda(agg, cam, vt, N_VPL, rzk.CLAMP_RADIANCE, tau, rzk.mrcs_params(seed=VPL_SEED))
+    setup_s = time.perf_counter() - t0
+    info = m.info()
+    _, _, reps, _ = m.clusters()
+    n_reps = int((reps >= 0).sum())
+    out = torch.empty((cam.n_pixels, 3), dtype=torch.float32, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def step():
+        m.gather(recv, cam.n_pixels, scale=1.0 / num_emitted, out=out, image_width=WIDTH)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    times = []
+    with ClockSampler(0) as clk:
+        for _ in range(args.steps):
+            flush.fill_(1)
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            step()
+            b.record(stream)
+            b.synchronize()
+            times.append(a.elapsed_time(b) / 1e3)
+    ctx.check()
+    launches_step = kernels_per_call(step)
+    ms = 1e3 * sum(times) / len(times)
+    evals = cam.n_pixels * n_reps
+    line = {
+        "metric": "MRCS clustered-gather evals/s (pixel x cluster representative, shadow ray each)",
+        "value": evals / (ms / 1e3), "unit": "evals/s", "n_gpus": 1, "steps": len(times),
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "mrcs_room_objects_300k_tris_512x512_32768_vpls",
+                   "rows": info["rows"], "columns": info["columns"], "num_clusters": info["num_clusters"],
+                   "representatives": n_reps, "evals_per_step": evals, "block_size": 32,
+                   "l2": "flushed between timed steps (256 MiB write)"},
+        "setup_s": setup_s,
+        "setup_stage_ms": dict(zip(["pixels_and_columns", "reduced_matrix", "clustering", "representatives"],
+                                   info["stage_ms"])),
+        "clocks": clk.summary(), "gpu_launches": launches_step * len(times),
+        "gpu_launches_note": f"{launches_step} kernels per step, counted as the kernel nodes of one captured step",
+        "image_finite": bool(torch.isfinite(out).all()), "tau": tau,
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def run_lightslice(args):
     """LightSlice on the scaled scene: 512 x 512 shading points, the first 32,768 VPLs (those
     of bounce <= 1 are clustered), slices of at most 1,024 points (~256), 1,000 global
@@ -784,10 +858,12 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="scaled", choices=["scaled", "batch", "lightslice", "guided", "serve"],
+    ap.add_argument("--workload", default="scaled",
+                    choices=["scaled", "batch", "lightslice", "mrcs", "guided", "serve"],
                     help="scaled: the 512x512 x 32,768-VPL gather (default); batch: 64 uneven "
                          "instances, batched + graph vs plain launches (1 GPU); lightslice: "
-                         "LightSlice build + clustered gather on the scaled scene (1 GPU); guided: "
+                         "LightSlice build + clustered gather on the scaled scene (1 GPU); mrcs: matrix "
+                         "row-column sampling set-up + clustered gather on the scaled scene (1 GPU); guided: "
                          "LightSlice-guided path tracing, 1024^2 x 16 spp (1 GPU)")
     ap.add_argument("--spp", type=int, default=16)
     ap.add_argument("--side", type=int, default=1024)
@@ -811,6 +887,8 @@ def main():
         return run_batch(args)
     if args.workload == "lightslice":
         return run_lightslice(args)
+    if args.workload == "mrcs":
+        return run_mrcs(args)
     if args.workload == "guided":
         return run_guided(args)
     if args.workload == "serve":

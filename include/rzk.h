@@ -260,6 +260,49 @@ rzk_status rzk_cluster_by_sampling(const float *d_matrix, int rows, int cols, in
                                    int32_t *h_representative, float *h_weight,
                                    int32_t *h_assign, void *stream);
 
+/* Matrix row-column sampling ---------------------------------------------------------- */
+
+/* MatrixRowColumnSampling (mrcs.cc:16-186, mrcs.h:17-45). */
+typedef struct rzk_mrcs rzk_mrcs;
+typedef struct {
+    int32_t block_size;     /* side of the pixel strata that give the matrix rows (32) */
+    float cluster_ratio;    /* clusters per VPL (0.01) */
+    int32_t max_clusters;   /* cap on the cluster count (1000) */
+    int32_t max_columns;    /* more VPLs than this are resampled to this many columns (10000) */
+    uint32_t seed;          /* the set-up's random stream is (seed, 7, 0) */
+} rzk_mrcs_params;
+
+/* MatrixRowColumnSampling's defaults (mrcs.cc:16-20; max_columns mrcs.cc:79). */
+rzk_status rzk_mrcs_params_default(rzk_mrcs_params *params);
+/* MatrixRowColumnSampling::initialize (mrcs.cc:43-186) for the camera's image and the
+ * device VPLs: stratified pixels (ImageSampler::sample_stratified, image_sampler.cc:8-23),
+ * the columns (every VPL, or max_columns resampled by average power), the reduced matrix
+ * (LightTransportMatrix::fill) on the device, then ClusterBuilder::cluster_by_sampling.
+ * All draws come from one stream in the reference's program order.  With more than
+ * max_columns VPLs the reference assigns columns past the end of its reduced matrix and
+ * gathers from all_vpls with reduced indices (cluster_builder.cc:189-199, mrcs.cc:36);
+ * here the clustering and the representatives use the resampled columns.  The VPLs need
+ * not outlive the call.  Synchronises `stream`. */
+rzk_status rzk_mrcs_create(rzk_context *ctx, rzk_scene *scene, const rzk_camera *camera,
+                           const rzk_vpl *d_vpls, int n_vpl, int clamp_mode, float tau,
+                           const rzk_mrcs_params *params, void *stream, rzk_mrcs **out);
+rzk_status rzk_mrcs_destroy(rzk_mrcs *mrcs);
+/* Matrix rows (sampled pixels), columns, the target cluster count, the clusters found
+ * (before dropping those without a representative) and the set-up stage times in ms
+ * (pixels + columns, matrix, clustering, representatives).  Any pointer may be NULL. */
+rzk_status rzk_mrcs_info(const rzk_mrcs *mrcs, int *n_rows, int *n_columns, int *num_clusters,
+                         int *n_clusters, float *stage_ms);
+/* The sampled pixels (x, y per row) and per cluster its centre column, representative
+ * column (-1: none, the cluster never gathers) and weight.  Any pointer may be NULL. */
+rzk_status rzk_mrcs_clusters(const rzk_mrcs *mrcs, int32_t *h_pixels, int32_t *h_center,
+                             int32_t *h_representative, float *h_weight);
+/* MatrixRowColumnSampling::gather_clusters (mrcs.cc:28-41) for every receiver:
+ * d_rgb[r] = scale * sum over clusters of weight x radiance(r, representative), added in
+ * cluster order (the integrator divides by num_emitted_photons, vpl.cc:481-484: pass
+ * scale = 1 / num_emitted).  image_width as in rzk_gather_cfg. */
+rzk_status rzk_mrcs_gather(rzk_mrcs *mrcs, const rzk_receiver *d_recv, int n_recv, int image_width,
+                           float scale, float *d_rgb, void *stream);
+
 /* LightSlice ------------------------------------------------------------------------- */
 
 /* LightSlice's settings (lightslice.h:306-312, lightslice.cc:23-85). */

@@ -278,6 +278,8 @@ class RefHarness:
             L.rref_ls_maps.argtypes = [P, P, P, P, P]
             L.rref_ls_gather.argtypes = [P, P, I32, I32, F32, P]
             L.rref_ls_guided.argtypes = [P, P, I32, I32, I32, I32, F32, I32, U32, P]
+            L.rref_mrcs.restype = I32
+            L.rref_mrcs.argtypes = [P, P, I32, I32, F32, U32, I32, F32, I32, P, I32, P, P, P, P, I32]
             cls._lib = L
         return cls._lib
 
@@ -371,6 +373,22 @@ class RefHarness:
         n = self.lib().rref_cluster_by_sampling(self.h, _ptr(mat), rows, cols, num_clusters, seed,
                                                 _ptr(c), _ptr(r), _ptr(w), _ptr(a))
         return c[:n], r[:n], w[:n], a
+
+    def mrcs(self, vpls, clamp_mode, tau, seed, recv, block_size=32, cluster_ratio=0.01, max_clusters=1000):
+        """The reference's MatrixRowColumnSampling::initialize on `vpls` (its draws from the
+        stream (seed, 7, 0)), then gather_clusters for every receiver (unscaled).  Returns
+        (image [n, 3], centres, representatives, weights)."""
+        vpls = np.ascontiguousarray(vpls)
+        recv = np.ascontiguousarray(recv)
+        n = recv.shape[0]
+        out = np.zeros((n, 3), np.float32)
+        cap = max(1, vpls.shape[0])
+        c = np.zeros(cap, np.int32); r = np.zeros(cap, np.int32); w = np.zeros(cap, np.float32)
+        k = self.lib().rref_mrcs(self.h, _ptr(vpls), vpls.shape[0], clamp_mode, tau, seed, block_size,
+                                 cluster_ratio, max_clusters, _ptr(recv), n, _ptr(out), _ptr(c), _ptr(r),
+                                 _ptr(w), cap)
+        k = min(k, cap)
+        return out, c[:k], r[:k], w[:k]
 
     def incident(self, recv, vpls, clamp_mode, tau):
         n, m = recv.shape[0], vpls.shape[0]

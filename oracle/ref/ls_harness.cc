@@ -82,21 +82,6 @@ using namespace rref;
 
 namespace {
 
-/* The evaluator LightSlice calls: VirtualPointLight's radiance and incident radiance, as
- * restated in ref_harness.cc against the reference's own types. */
-struct HarnessEval : public IVirtualPointLightEvaluator {
-    RefScene *s = nullptr;
-    int mode = 0, inc_mode = 0;
-    float tau = 0.0f, inc_tau = 0.0f;
-    Rgb radiance(Scene *, const Receiver &r, const BrdfPointLight &l, bool &visible) override {
-        LocalGeometry dg(r);
-        return gather_point(s, dg, r.wo, r.m, &l, mode, tau, visible);
-    }
-    Rgb incident_radiance(Scene *, const Receiver &r, const BrdfPointLight &l) override {
-        return rref::incident_radiance(r, l, inc_mode, inc_tau);
-    }
-};
-
 struct RefLs {
     RefScene *s = nullptr;
     LightSlice *ls = nullptr;

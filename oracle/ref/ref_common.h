@@ -83,6 +83,22 @@ BrdfPointLight to_vpl(const RefScene *s, const rzk_vpl &v);
 Rgb gather_point(const RefScene *s, const LocalGeometry &dg, const Vec3 &wo, Material *m,
                  const BrdfPointLight *vpl, int clamp_mode, Float clamp_threshold, bool &visible);
 Rgb incident_radiance(const Receiver &r, const BrdfPointLight &vpl, int clamp_mode, Float threshold);
+
+/* The evaluator that LightSlice and MatrixRowColumnSampling call: VirtualPointLight's
+ * radiance and incident radiance, as restated in ref_harness.cc against the reference's
+ * own types. */
+struct HarnessEval : public IVirtualPointLightEvaluator {
+    RefScene *s = nullptr;
+    int mode = 0, inc_mode = 0;
+    float tau = 0.0f, inc_tau = 0.0f;
+    Rgb radiance(Scene *, const Receiver &r, const BrdfPointLight &l, bool &visible) override {
+        LocalGeometry dg(r);
+        return gather_point(s, dg, r.wo, r.m, &l, mode, tau, visible);
+    }
+    Rgb incident_radiance(Scene *, const Receiver &r, const BrdfPointLight &l) override {
+        return rref::incident_radiance(r, l, inc_mode, inc_tau);
+    }
+};
 void fill_receiver(const Ray &r, const HitRecord &rec, rzk_receiver &out, const RefScene *s);
 
 }  // namespace rref

@@ -181,13 +181,20 @@ rzk_status ltm_alphas(const float *mat, int rows, int cols, float *alphas, float
 rzk_status cluster_by_sampling(const float *mat, int rows, int cols, int num_clusters, uint32_t seed,
                                int *h_n, int32_t *h_center, int32_t *h_rep, float *h_weight,
                                int32_t *h_assign, cudaStream_t st, float *h_mags) {
+    HostRng g{seed, 1u, 0u};
+    return cluster_by_sampling(mat, rows, cols, num_clusters, g, h_n, h_center, h_rep, h_weight, h_assign, st,
+                               h_mags);
+}
+
+rzk_status cluster_by_sampling(const float *mat, int rows, int cols, int num_clusters, HostRng &g, int *h_n,
+                               int32_t *h_center, int32_t *h_rep, float *h_weight, int32_t *h_assign,
+                               cudaStream_t st, float *h_mags) {
     for (int j = 0; j < cols; ++j) h_assign[j] = -1;
     if (cols < num_clusters) {   // cluster_builder.cc:90-101
         for (int i = 0; i < cols; ++i) { h_center[i] = i; h_weight[i] = 1.0f; h_rep[i] = -1; }
         *h_n = cols;
         return RZK_OK;
     }
-    HostRng g{seed, 1u, 0u};
     DevBuf<float> alphas;
     RZK_CUDA_TRY(alphas.alloc(cols));
     rzk_status e = ltm_alphas(mat, rows, cols, alphas.p, nullptr, st);

@@ -3,6 +3,7 @@
 #define RZK_CLUSTER_CUH_
 
 #include "rzk_internal.cuh"
+#include "rzk_hostutil.h"
 
 namespace rzk {
 
@@ -14,6 +15,11 @@ rzk_status ltm_alphas(const float *mat, int rows, int cols, float *alphas, float
 rzk_status cluster_by_sampling(const float *mat, int rows, int cols, int num_clusters, uint32_t seed,
                                int *h_n, int32_t *h_center, int32_t *h_rep, float *h_weight,
                                int32_t *h_assign, cudaStream_t st, float *h_mags = nullptr);
+// The same, drawing from a stream the caller has already advanced (the reference draws
+// the clustering from the scene's one stream after whatever came before it).
+rzk_status cluster_by_sampling(const float *mat, int rows, int cols, int num_clusters, HostRng &g, int *h_n,
+                               int32_t *h_center, int32_t *h_rep, float *h_weight, int32_t *h_assign,
+                               cudaStream_t st, float *h_mags = nullptr);
 
 }  // namespace rzk
 

@@ -64,6 +64,12 @@ SIGNATURES = [
     ("rzk_gather_noalloc", I32, [P, P, I32, I32, P, I32, I32, F32, F32, P, P]),
     ("rzk_ltm_alphas", I32, [P, I32, I32, P, P, P]),
     ("rzk_cluster_by_sampling", I32, [P, I32, I32, I32, U32, P, P, P, P, P, P]),
+    ("rzk_mrcs_params_default", I32, [P]),
+    ("rzk_mrcs_create", I32, [P, P, P, P, I32, I32, F32, P, P, P]),
+    ("rzk_mrcs_destroy", I32, [P]),
+    ("rzk_mrcs_info", I32, [P, P, P, P, P, P]),
+    ("rzk_mrcs_clusters", I32, [P, P, P, P, P]),
+    ("rzk_mrcs_gather", I32, [P, P, I32, I32, F32, P, P]),
     ("rzk_batch_variants", I32, []),
     ("rzk_batch_create", I32, [P, P, I32, I32, I32, P]),
     ("rzk_batch_run", I32, [P, P]),
@@ -401,6 +407,76 @@ class ClusterBuilderCuda:
                                                _stream_ptr(stream)), "rzk_cluster_by_sampling")
         k = n.value
         return c[:k], r[:k], w[:k], a[:cols]
+
+
+class MrcsParamsC(ctypes.Structure):
+    """ctypes mirror of rzk_mrcs_params."""
+    _fields_ = [("block_size", I32), ("cluster_ratio", F32), ("max_clusters", I32), ("max_columns", I32),
+                ("seed", U32)]
+
+
+def mrcs_params(**kw) -> MrcsParamsC:
+    """MatrixRowColumnSampling's defaults (mrcs.cc:16-20) with keyword overrides."""
+    p = MrcsParamsC()
+    check(load().rzk_mrcs_params_default(ctypes.byref(p)), "rzk_mrcs_params_default")
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+class MrcsCuda:
+    """MatrixRowColumnSampling (mrcs.h:17-45): initialize() at construction on device VPLs,
+    gather_clusters() for every receiver with gather()."""
+
+    def __init__(self, agg: "AggregateCuda", camera: "Camera", vpls, n_vpl: int, clamp_mode: int, tau: float,
+                 params: MrcsParamsC | None = None, stream=None):
+        self.lib = load()
+        self.agg = agg
+        self.params = params or mrcs_params()
+        h = ctypes.c_void_p()
+        check(self.lib.rzk_mrcs_create(agg.ctx.h, agg.h, camera.rec.ctypes.data, _dptr(vpls) if n_vpl else None,
+                                       n_vpl, clamp_mode, tau, ctypes.byref(self.params),
+                                       _stream_ptr(stream), ctypes.byref(h)), "rzk_mrcs_create")
+        self.h = h
+
+    def info(self) -> dict:
+        rows, cols, target, n = I32(), I32(), I32(), I32()
+        ms = np.zeros(4, np.float32)
+        check(self.lib.rzk_mrcs_info(self.h, ctypes.byref(rows), ctypes.byref(cols), ctypes.byref(target),
+                                     ctypes.byref(n), ms.ctypes.data), "rzk_mrcs_info")
+        return {"rows": rows.value, "columns": cols.value, "num_clusters": target.value, "clusters": n.value,
+                "stage_ms": ms.tolist()}
+
+    def clusters(self):
+        """(pixels [rows, 2] (x, y), centres, representatives, weights)."""
+        i = self.info()
+        px = np.zeros((i["rows"], 2), np.int32)
+        c = np.zeros(max(i["clusters"], 1), np.int32)
+        r = np.zeros_like(c)
+        w = np.zeros(c.shape[0], np.float32)
+        check(self.lib.rzk_mrcs_clusters(self.h, px.ctypes.data, c.ctypes.data, r.ctypes.data, w.ctypes.data),
+              "rzk_mrcs_clusters")
+        k = i["clusters"]
+        return px, c[:k], r[:k], w[:k]
+
+    def gather(self, recv, n_recv, scale=1.0, out=None, image_width=0, stream=None):
+        torch = _torch()
+        if out is None:
+            out = torch.empty((n_recv, 3), dtype=torch.float32, device="cuda")
+        check(self.lib.rzk_mrcs_gather(self.h, _dptr(recv), n_recv, image_width, scale, _dptr(out),
+                                       _stream_ptr(stream)), "rzk_mrcs_gather")
+        return out
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.rzk_mrcs_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class GatherJobC(ctypes.Structure):

@@ -63,3 +63,20 @@ def test_new_entry_points_reject_bad_arguments_without_gpu():
     assert lib.rzk_batch_create(None, None, 0, 0, 0, None) == rzk.ERR_INVALID
     p = rzk.lightslice_params()
     assert p.num_clusters == 600 and p.max_slice_size == 256 and p.num_neighbor_slices == 16
+
+
+def test_mrcs_entry_points_reject_bad_arguments_without_gpu():
+    import ctypes
+    from renzoku_b200 import rzk
+    lib = rzk.load()
+    p = rzk.mrcs_params()
+    # MatrixRowColumnSampling's defaults (mrcs.cc:16-20, 79)
+    assert (p.block_size, p.max_clusters, p.max_columns) == (32, 1000, 10000)
+    assert abs(p.cluster_ratio - 0.01) < 1e-9
+    assert lib.rzk_mrcs_params_default(None) == rzk.ERR_INVALID
+    out = ctypes.c_void_p()
+    assert lib.rzk_mrcs_create(None, None, None, None, 0, 0, 0.0, ctypes.byref(p), None,
+                               ctypes.byref(out)) == rzk.ERR_INVALID
+    assert lib.rzk_mrcs_gather(None, None, 0, 0, 1.0, None, None) == rzk.ERR_INVALID
+    assert lib.rzk_mrcs_info(None, None, None, None, None, None) == rzk.ERR_INVALID
+    assert lib.rzk_mrcs_destroy(None) == rzk.ERR_INVALID
