@@ -503,6 +503,56 @@ def run_batch(args):
     return 0
 
 
+def run_restart(args):
+    """Warm restart of device scenes: the time to build a scene from its description
+    (upload, LBVH, SAH any-hit tree, lights) against the time to restore it from a blob
+    of its device arrays (rzk_scene_deserialize), for the scaled scene (~300k triangles)
+    and the sphere scene (~960k triangles); each restored scene is checked against the
+    built one (BVH bytes).  Prints one JSON line."""
+    import torch
+    from renzoku_b200 import build as rbuild
+    rbuild.build()
+    from renzoku_b200 import rzk, scenegen as sg
+    ctx = rzk.Context(0)
+    rows = []
+    for name, sc in (("room_objects_300k", sg.room_objects(2000, WIDTH, HEIGHT)),
+                     ("room_spheres_960k", sg.room_spheres(20000, 1024, 1024))):
+        rzk.AggregateCuda(ctx, sc).close()   # first-use costs (module load, pools) outside the timing
+        build, save, restore = [], [], []
+        for _ in range(max(1, args.steps)):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            agg = rzk.AggregateCuda(ctx, sc)
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            blob = agg.serialize()
+            t2 = time.perf_counter()
+            back = rzk.AggregateCuda.restore(ctx, blob, sc)
+            torch.cuda.synchronize()
+            t3 = time.perf_counter()
+            build.append(t1 - t0)
+            save.append(t2 - t1)
+            restore.append(t3 - t2)
+            same = all(x.tobytes() == y.tobytes() for x, y in zip(agg.bvh_dump(), back.bvh_dump()))
+            agg.close()
+            back.close()
+        rows.append({"scene": name, "triangles": back.n_tris, "blob_bytes": len(blob),
+                     "build_ms": 1e3 * min(build), "serialize_ms": 1e3 * min(save),
+                     "restore_ms": 1e3 * min(restore), "restore_speedup": min(build) / min(restore),
+                     "bvh_identical": same})
+    ctx.check()
+    line = {
+        "metric": "scene restore time (ms, 960k-triangle scene, from a host blob)",
+        "value": rows[-1]["restore_ms"], "unit": "ms", "n_gpus": 1, "steps": max(1, args.steps), "warmup": 1,
+        "ms_per_step": rows[-1]["restore_ms"], "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "scene_warm_restart_300k_960k_tris", "timing": "host wall clock, min over steps"},
+        "scenes": rows,
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def run_mrcs(args):
     """Matrix row-column sampling on the scaled scene: 512 x 512 shading points, the first
     32,768 VPLs resampled by power to 10,000 columns, 256 stratified rows (32 x 32 strata),
@@ -859,11 +909,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="scaled",
-                    choices=["scaled", "batch", "lightslice", "mrcs", "guided", "serve"],
+                    choices=["scaled", "batch", "lightslice", "mrcs", "guided", "serve", "restart"],
                     help="scaled: the 512x512 x 32,768-VPL gather (default); batch: 64 uneven "
                          "instances, batched + graph vs plain launches (1 GPU); lightslice: "
                          "LightSlice build + clustered gather on the scaled scene (1 GPU); mrcs: matrix "
-                         "row-column sampling set-up + clustered gather on the scaled scene (1 GPU); guided: "
+                         "row-column sampling set-up + clustered gather on the scaled scene (1 GPU); restart: "
+                         "scene build vs restore from a blob (1 GPU); guided: "
                          "LightSlice-guided path tracing, 1024^2 x 16 spp (1 GPU)")
     ap.add_argument("--spp", type=int, default=16)
     ap.add_argument("--side", type=int, default=1024)
@@ -889,6 +940,8 @@ def main():
         return run_lightslice(args)
     if args.workload == "mrcs":
         return run_mrcs(args)
+    if args.workload == "restart":
+        return run_restart(args)
     if args.workload == "guided":
         return run_guided(args)
     if args.workload == "serve":

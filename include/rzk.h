@@ -100,6 +100,31 @@ rzk_status rzk_camera_setup(const float eye[3], const float lookat[3], const flo
                             float fov_deg, int width, int height, float film_w, float film_h,
                             rzk_camera *h_out);
 
+/* Warm restart: a built scene as one host blob (device arrays and host-side counts), and
+ * back.  No reference counterpart (the reference rebuilds its BVH from the scene file on
+ * every run, aggregate_bvh.cc:48-240).  A restored scene answers every query bit for bit
+ * like the scene it was saved from, on any device of the same architecture. */
+rzk_status rzk_scene_serialized_size(rzk_scene *scene, size_t *bytes);
+/* Copies the scene into h_buf (cap bytes, at least rzk_scene_serialized_size); *written =
+ * bytes used.  Synchronises `stream`. */
+rzk_status rzk_scene_serialize(rzk_scene *scene, void *h_buf, size_t cap, size_t *written, void *stream);
+/* A new scene on ctx's device from a blob; RZK_ERR_INVALID for a blob that is not one (bad
+ * magic or version, truncated, sizes that disagree with its counts).  Synchronises
+ * `stream`. */
+rzk_status rzk_scene_deserialize(rzk_context *ctx, const void *h_buf, size_t size, void *stream,
+                                 rzk_scene **out);
+
+/* Transport-matrix files in MatrixC<Rgb>::save's format (matrix_c.cc:6-23): the text
+ * header "rows cols\n" then every entry's RGB floats column by column - the device layout
+ * [cols][rows][3] of rzk_gather_matrix.  rzk_matrix_save writes d_matrix to `path`;
+ * rzk_matrix_file_info reads the header; rzk_matrix_load reads a file whose header matches
+ * rows x cols into d_matrix (MatrixC::load reads every entry into its first element and
+ * stores an unset value, matrix_c.cc:38-41; this reads what save wrote).  Synchronise
+ * `stream`. */
+rzk_status rzk_matrix_save(const char *path, const float *d_matrix, int rows, int cols, void *stream);
+rzk_status rzk_matrix_file_info(const char *path, int *rows, int *cols);
+rzk_status rzk_matrix_load(const char *path, float *d_matrix, int rows, int cols, void *stream);
+
 /* IVplGenerator ----------------------------------------------------------------------- */
 
 /* VplGenerator::spawn (vpl_generator.cc:183-204; generate_vpl 127-181, trace_vpl 43-110;

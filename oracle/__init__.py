@@ -278,6 +278,7 @@ class RefHarness:
             L.rref_ls_maps.argtypes = [P, P, P, P, P]
             L.rref_ls_gather.argtypes = [P, P, I32, I32, F32, P]
             L.rref_ls_guided.argtypes = [P, P, I32, I32, I32, I32, F32, I32, U32, P]
+            L.rref_matrix_save.argtypes = [P, I32, I32, ctypes.c_char_p]
             L.rref_mrcs.restype = I32
             L.rref_mrcs.argtypes = [P, P, I32, I32, F32, U32, I32, F32, I32, P, I32, P, P, P, P, I32]
             cls._lib = L
@@ -373,6 +374,12 @@ class RefHarness:
         n = self.lib().rref_cluster_by_sampling(self.h, _ptr(mat), rows, cols, num_clusters, seed,
                                                 _ptr(c), _ptr(r), _ptr(w), _ptr(a))
         return c[:n], r[:n], w[:n], a
+
+    @classmethod
+    def matrix_save(cls, mat, path):
+        """The reference's LightTransportMatrix::save of a column-major matrix [cols, rows, 3]."""
+        mat = np.ascontiguousarray(mat, np.float32)
+        cls.lib().rref_matrix_save(_ptr(mat), mat.shape[1], mat.shape[0], str(path).encode())
 
     def mrcs(self, vpls, clamp_mode, tau, seed, recv, block_size=32, cluster_ratio=0.01, max_clusters=1000):
         """The reference's MatrixRowColumnSampling::initialize on `vpls` (its draws from the

@@ -457,6 +457,14 @@ void rref_ltm_alphas(const float *mat, int rows, int cols, float *alphas, float 
     delete R;
 }
 
+/* LightTransportMatrix::save -> MatrixC<Rgb>::save (light_transport_matrix.cc:144-146,
+ * matrix_c.cc:6-23) of a column-major matrix [cols][rows][3]. */
+void rref_matrix_save(const float *mat, int rows, int cols, const char *path) {
+    LightTransportMatrix *R = make_ltm(mat, rows, cols);
+    R->save(path);
+    delete R;
+}
+
 /* ClusterBuilder::cluster_by_sampling (cluster_builder.cc:82-273) with its random draws from
  * stream (seed, 1, 0).  Outputs the final clusters in order and, per column, the index of
  * the final cluster holding it (-1 if none).  Returns the number of clusters. */

@@ -47,6 +47,12 @@ SIGNATURES = [
     ("rzk_scene_info", I32, [P, P, P, P, P]),
     ("rzk_scene_bounding_box", I32, [P, P]),
     ("rzk_scene_rebuild", I32, [P, P]),
+    ("rzk_scene_serialized_size", I32, [P, P]),
+    ("rzk_scene_serialize", I32, [P, P, ctypes.c_size_t, P, P]),
+    ("rzk_scene_deserialize", I32, [P, P, ctypes.c_size_t, P, P]),
+    ("rzk_matrix_save", I32, [ctypes.c_char_p, P, I32, I32, P]),
+    ("rzk_matrix_file_info", I32, [ctypes.c_char_p, P, P]),
+    ("rzk_matrix_load", I32, [ctypes.c_char_p, P, I32, I32, P]),
     ("rzk_bvh_dump", I32, [P, P, P, P, I32, P]),
     ("rzk_morton_codes", I32, [P, P, P]),
     ("rzk_occluded_batch", I32, [P, P, P, I32, P, P]),
@@ -219,12 +225,39 @@ class AggregateCuda:
         check(self.lib.rzk_scene_create(ctx.h, ctypes.byref(self._desc), _stream_ptr(stream),
                                         ctypes.byref(h)), "rzk_scene_create")
         self.h = h
+        self._info()
+        self.tmin = scene.tmin
+
+    def _info(self):
         nt, nn, nl = I32(), I32(), I32()
         nb = ctypes.c_size_t()
-        check(self.lib.rzk_scene_info(h, ctypes.byref(nt), ctypes.byref(nn), ctypes.byref(nl),
+        check(self.lib.rzk_scene_info(self.h, ctypes.byref(nt), ctypes.byref(nn), ctypes.byref(nl),
                                       ctypes.byref(nb)), "rzk_scene_info")
         self.n_tris, self.n_nodes, self.n_levels, self.device_bytes = nt.value, nn.value, nl.value, nb.value
+
+    def serialize(self, stream=None) -> bytes:
+        """The built scene as one blob (rzk_scene_serialize), for a warm restart."""
+        n = ctypes.c_size_t()
+        check(self.lib.rzk_scene_serialized_size(self.h, ctypes.byref(n)), "rzk_scene_serialized_size")
+        buf = ctypes.create_string_buffer(n.value)
+        w = ctypes.c_size_t()
+        check(self.lib.rzk_scene_serialize(self.h, buf, n.value, ctypes.byref(w), _stream_ptr(stream)),
+              "rzk_scene_serialize")
+        return buf.raw[: w.value]
+
+    @classmethod
+    def restore(cls, ctx: Context, blob: bytes, scene: sg.Scene, stream=None) -> "AggregateCuda":
+        """A scene rebuilt from serialize()'s blob without building its trees again; `scene`
+        is the description it was made from (kept for the Python-side fields)."""
+        self = cls.__new__(cls)
+        self.ctx, self.lib, self.scene = ctx, ctx.lib, scene
+        h = ctypes.c_void_p()
+        check(self.lib.rzk_scene_deserialize(ctx.h, blob, len(blob), _stream_ptr(stream), ctypes.byref(h)),
+              "rzk_scene_deserialize")
+        self.h = h
+        self._info()
         self.tmin = scene.tmin
+        return self
 
     def close(self):
         if getattr(self, "h", None):
@@ -375,6 +408,24 @@ def pair_indices(seed: int, n_pairs: int, n_recv: int, n_vpl: int, draw_u32):
     ri = np.array([draw_u32(seed, 3, k, 0) % n_recv for k in range(n_pairs)], np.int32)
     vi = np.array([draw_u32(seed, 3, k, 1) % n_vpl for k in range(n_pairs)], np.int32)
     return ri, vi
+
+
+def matrix_save(path: str, mat, stream=None) -> None:
+    """Writes a device matrix [cols, rows, 3] in MatrixC<Rgb>::save's format."""
+    check(load().rzk_matrix_save(str(path).encode(), _dptr(mat), mat.shape[1], mat.shape[0],
+                                 _stream_ptr(stream)), "rzk_matrix_save")
+
+
+def matrix_load(path: str, stream=None):
+    """Reads a MatrixC<Rgb>::save file into a new device matrix [cols, rows, 3]."""
+    torch = _torch()
+    rows, cols = I32(), I32()
+    check(load().rzk_matrix_file_info(str(path).encode(), ctypes.byref(rows), ctypes.byref(cols)),
+          "rzk_matrix_file_info")
+    mat = torch.empty((cols.value, rows.value, 3), dtype=torch.float32, device="cuda")
+    check(load().rzk_matrix_load(str(path).encode(), _dptr(mat), rows.value, cols.value, _stream_ptr(stream)),
+          "rzk_matrix_load")
+    return mat
 
 
 class ClusterBuilderCuda:

@@ -80,3 +80,25 @@ def test_mrcs_entry_points_reject_bad_arguments_without_gpu():
     assert lib.rzk_mrcs_gather(None, None, 0, 0, 1.0, None, None) == rzk.ERR_INVALID
     assert lib.rzk_mrcs_info(None, None, None, None, None, None) == rzk.ERR_INVALID
     assert lib.rzk_mrcs_destroy(None) == rzk.ERR_INVALID
+
+
+def test_matrix_header_reader_without_gpu(oracle_built, tmp_path):
+    """rzk_matrix_file_info reads the header of a file the reference's own
+    LightTransportMatrix::save wrote (host code only), and rejects a damaged one."""
+    import ctypes
+    import numpy as np
+    from oracle import RefHarness
+    from renzoku_b200 import rzk
+    lib = rzk.load()
+    m = np.random.default_rng(1).random((9, 4, 3)).astype(np.float32)   # 9 columns x 4 rows
+    path = tmp_path / "m.bin"
+    RefHarness.matrix_save(m, str(path))
+    rows, cols = ctypes.c_int32(), ctypes.c_int32()
+    assert lib.rzk_matrix_file_info(str(path).encode(), ctypes.byref(rows), ctypes.byref(cols)) == rzk.OK
+    assert (rows.value, cols.value) == (4, 9)
+    bad = tmp_path / "bad.bin"
+    bad.write_bytes(b"4 x\n" + m.tobytes())
+    assert lib.rzk_matrix_file_info(str(bad).encode(), ctypes.byref(rows), ctypes.byref(cols)) == rzk.ERR_INVALID
+    assert lib.rzk_matrix_file_info(str(tmp_path / "none").encode(), ctypes.byref(rows),
+                                    ctypes.byref(cols)) == rzk.ERR_INVALID
+    assert lib.rzk_scene_deserialize(None, b"RZKSCN01", 8, None, ctypes.byref(ctypes.c_void_p())) == rzk.ERR_INVALID
