@@ -60,6 +60,36 @@ def _dist():
     return ws, rank, local
 
 
+def init_ranks(backend: str = "nccl", timeout_s: int = 120):
+    """One process per GPU under torchrun: the process group (None for a single process),
+    rendezvous on 127.0.0.1, with a short timeout so that a rank that never arrives ends the
+    others' collectives with an error."""
+    ws, _, _ = _dist()
+    if ws <= 1:
+        return None
+    import datetime
+    import torch.distributed as dist
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
+    return dist
+
+
+def max_over_ranks(pg, x: float, device) -> float:
+    """The largest x over all ranks (every rank gets it); x itself without a group."""
+    if pg is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world_size: int, units_per_rank_step: float, steps: int, max_seconds: float) -> float:
+    """Whole-job throughput of replicas: every rank processes units_per_rank_step per step,
+    the job takes as long as its slowest rank."""
+    return world_size * units_per_rank_step * steps / max_seconds
+
+
 class ClockSampler:
     """nvidia-smi clock / throttle-reason samples while the timed region runs."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -240,13 +270,7 @@ def run_ours(args):
     import torch
     ws, rank, local = _dist()
     torch.cuda.set_device(local)
-    pg = None
-    if ws > 1:
-        import datetime
-        import torch.distributed as dist
-        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-        pg = dist
+    pg = init_ranks("nccl")
     from renzoku_b200 import build as rbuild
     if rank == 0 or not os.path.exists(rbuild.LIB):
         rbuild.build()
@@ -300,14 +324,10 @@ def run_ours(args):
         torch.cuda.synchronize()
     if pg:
         pg.barrier()
-    total = sum(times)
-    if pg:
-        t = torch.tensor([total], device="cuda", dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        total = float(t.item())
+    total = max_over_ranks(pg, sum(times), "cuda")
     ctx.check()
     evals_step = n_recv * N_VPL
-    value = ws * evals_step * len(times) / total
+    value = job_rate(ws, evals_step, len(times), total)
     launches_step = kernels_per_call(step)
 
     # end to end through the public host-buffer call: receivers + VPLs from pinned host
@@ -332,11 +352,7 @@ def run_ours(args):
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         e2e_step()
-    e2e_s = (time.perf_counter() - t0) / e2e_steps
-    e2e_tensor = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-    if pg:
-        pg.all_reduce(e2e_tensor, op=pg.ReduceOp.MAX)
-    e2e_s = float(e2e_tensor.item())
+    e2e_s = max_over_ranks(pg, (time.perf_counter() - t0) / e2e_steps, "cuda")
     img_ok = bool(torch.isfinite(img_h).all()) and float(img_h.sum()) > 0
 
     line = None
