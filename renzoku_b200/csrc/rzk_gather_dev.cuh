@@ -330,4 +330,96 @@ __device__ __forceinline__ bool gather_item(const DevScene &s, const rzk_receive
     return true;
 }
 
+// Visibility half of gather_item, for gathers split into a tracing pass and a summing
+// pass: the 32 receivers of warp tile `wt` against VPLs [j0, j1); masks[j - j0] = ballot of
+// the lanes whose pair's term is not exactly zero (pair_survives) and whose shadow segment
+// is unoccluded - exactly the pairs gather_item adds.  Returns false if a bounded wait gave
+// up (reported in the error word).
+template <int TILE>
+__device__ __forceinline__ bool visibility_item(const DevScene &s, const rzk_receiver *recv, int n_recv,
+                                                const rzk_vpl *vpls, int j0, int j1, int wt, WarpStage<TILE> &ws,
+                                                int lane, uint32_t *masks) {
+    const int ri = lane_receiver(wt, lane, n_recv, 0);
+    const int n_tiles = (j1 - j0 + TILE - 1) / TILE;
+    RecvRegs r;
+    r.p = mk(0.0f, 0.0f, 0.0f);
+    bool active = false;
+    if (ri >= 0) {
+        r = load_receiver(recv + ri);
+        active = r.mat >= 0;
+    }
+    if (n_tiles <= 0 || !__any_sync(kFull, active)) {
+        for (int j = j0 + lane; j < j1; j += 32) masks[j - j0] = 0u;
+        return true;
+    }
+    int occ_cache = -1;
+    if (lane == 0) {
+        int cnt = min(TILE, j1 - j0);
+        fence_proxy_async();
+        mbar_expect_tx(&ws.mb[0], cnt * (uint32_t)sizeof(rzk_vpl));
+        bulk_g2s(&ws.tl[0][0], vpls + j0, cnt * (uint32_t)sizeof(rzk_vpl), &ws.mb[0]);
+    }
+    for (int k = 0; k < n_tiles; ++k) {
+        const int buf = k & 1;
+        if (lane == 0 && k + 1 < n_tiles) {
+            int jn = j0 + (k + 1) * TILE;
+            int cnt = min(TILE, j1 - jn);
+            fence_proxy_async();
+            mbar_expect_tx(&ws.mb[buf ^ 1], cnt * (uint32_t)sizeof(rzk_vpl));
+            bulk_g2s(&ws.tl[buf ^ 1][0], vpls + jn, cnt * (uint32_t)sizeof(rzk_vpl), &ws.mb[buf ^ 1]);
+        }
+        bool ok = mbar_wait_bounded(&ws.mb[buf], ws.uses[buf] & 1u, lane == 0 ? s.err : nullptr);
+        ws.uses[buf]++;
+        if (__any_sync(kFull, !ok)) return false;
+        const rzk_vpl *tile = ws.tl[buf];
+        const int cnt = min(TILE, j1 - (j0 + k * TILE));
+        for (int v = 0; v < cnt; ++v) {
+            const rzk_vpl &l = tile[v];
+            PairGeo pg;
+            bool act = active && pair_survives(r, l, pg);
+            unsigned vis = 0u;
+            if (__any_sync(kFull, act)) {
+                Ray ray = make_ray(r.p, sub(pg.q, r.p));
+                float tmax = len(sub(pg.q, r.p)) - s.tmin;
+                vis = __ballot_sync(kFull, packet_visible_near(s, ray, tmax, act, ws.stk, occ_cache));
+            }
+            if (lane == 0) masks[k * TILE + v] = vis;
+        }
+        __syncwarp();
+    }
+    return true;
+}
+
+// Summing half: the 32 receivers of warp tile `wt` add, in VPL order, the terms of the
+// pairs that `masks` (one word per VPL, from visibility_item) marks - the same values in
+// the same order as gather_item with one chunk, so the sums are bit-identical to it.
+// WEIGHTED as in gather_item.  Writes partial[3 * ri ...].
+template <bool WEIGHTED>
+__device__ __forceinline__ void shade_item(const DevScene &s, const rzk_receiver *recv, int n_recv,
+                                           const rzk_vpl *vpls, int n_vpl, const uint32_t *masks, int wt, int mode,
+                                           float tau, float *partial, int lane, const float *weights) {
+    const int ri = lane_receiver(wt, lane, n_recv, 0);
+    if (ri < 0) return;
+    RecvRegs r = load_receiver(recv + ri);
+    Rgb sum = crgb(0.0f, 0.0f, 0.0f);
+    if (r.mat >= 0) {
+        const rzk_material rm = load_material(s.mats + r.mat);
+        const unsigned bit = 1u << lane;
+        for (int j = 0; j < n_vpl; ++j) {
+            if (!(masks[j] & bit)) continue;
+            const rzk_vpl &l = vpls[j];
+            PairGeo pg;
+            pair_survives(r, l, pg);
+            Rgb L = pair_radiance(s, r, rm, l, pg, mode, tau);
+            if (WEIGHTED) {
+                const float w = weights[j];
+                L = crgb(w * L.r, w * L.g, w * L.b);
+            }
+            sum = cadd(sum, L);
+        }
+    }
+    float *o = partial + 3 * (size_t)ri;
+    o[0] = sum.r; o[1] = sum.g; o[2] = sum.b;
+}
+
 }  // namespace rzk

@@ -143,7 +143,8 @@ __global__ void bin_keys_kernel(const int *slice, int n, int img_w, int mbits, u
 // cluster weight, summed in cluster order.  A pixel's sum does not depend on where its
 // bin placed it.
 struct SliceTables {
-    const int *tile_off;      // [n_slices + 1] first work item of each slice
+    const int *tile_off;      // [n_slices + 1] first work item of the slice at each position
+    const int *order;         // [n_slices] slice at each position: most representatives first
     const int *pix_off;       // [n_slices] first binned pixel
     const int *pix_cnt;       // [n_slices]
     const int *rep_off;       // [n_slices] first representative
@@ -153,10 +154,24 @@ struct SliceTables {
     int n_slices, n_items;
 };
 
+// The clustered gather runs in two passes so that its work splits finely without changing
+// any sum.  Tracing: items (slice position, 32-pixel tile, run of kVisChunk
+// representatives) - small and many, so the persistent warps finish together - each storing
+// one visibility ballot per representative.  Summing: one warp per tile adds
+// weight x radiance over its slice's representatives in cluster order for the pairs the
+// ballots mark, which are exactly the pairs (and the order) of a one-pass gather.
+constexpr int kVisChunk = 128;
+
+struct VisTables {
+    const int *vis_off;          // [n_slices + 1] first tracing item of the slice at each position
+    const long long *mask_off;   // [n_slices] first visibility word of the slice at each position
+    uint32_t *masks;             // per slice: [tile][representative]
+    int n_items;
+};
+
 template <int WARPS, int TILE, int MINB>
-__global__ void __launch_bounds__(WARPS * 32, MINB) cluster_gather_kernel(DevScene s, const rzk_receiver *recv,
-                                                                          SliceTables t, int mode, float tau,
-                                                                          float *sums, int *work) {
+__global__ void __launch_bounds__(WARPS * 32, MINB) cluster_vis_kernel(DevScene s, const rzk_receiver *recv,
+                                                                       SliceTables t, VisTables v, int *work) {
     __shared__ __align__(128) rzk_vpl tiles[WARPS][2][TILE];
     __shared__ __align__(8) uint64_t bar[WARPS][2];
     __shared__ int stacks[WARPS][STACK_CAP];
@@ -167,19 +182,41 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) cluster_gather_kernel(DevSce
         int item = 0;
         if (lane == 0) item = atomicAdd(work, 1);
         item = __shfl_sync(kFull, item, 0);
-        if (item >= t.n_items) break;
+        if (item >= v.n_items) break;
         int lo = 0, hi = t.n_slices - 1;
         while (lo < hi) {
             int mid = (lo + hi + 1) >> 1;
-            if (t.tile_off[mid] <= item) lo = mid; else hi = mid - 1;
+            if (v.vis_off[mid] <= item) lo = mid; else hi = mid - 1;
         }
-        const int sl = lo;
-        const int wt = item - t.tile_off[sl];
-        const int po = t.pix_off[sl], nr = t.pix_cnt[sl], ro = t.rep_off[sl], nc = t.rep_cnt[sl];
-        if (!gather_item<TILE, true>(s, recv + po, nr, 0, t.reps + ro, nc, 0, wt, nc, mode, tau,
-                                     sums + 3 * (size_t)po, ws, lane, t.weights + ro))
-            break;
+        const int sl = t.order[lo];
+        const int nc = t.rep_cnt[sl];
+        const int nch = (nc + kVisChunk - 1) / kVisChunk;
+        const int local = item - v.vis_off[lo];
+        const int wt = local / nch, c = local - wt * nch;
+        const int j0 = c * kVisChunk, j1 = min(nc, j0 + kVisChunk);
+        const int po = t.pix_off[sl], nr = t.pix_cnt[sl], ro = t.rep_off[sl];
+        uint32_t *m = v.masks + v.mask_off[lo] + (long long)wt * nc + j0;
+        if (!visibility_item<TILE>(s, recv + po, nr, t.reps + ro, j0, j1, wt, ws, lane, m)) break;
     }
+}
+
+constexpr int kShadeBlock = 128;
+
+__global__ void __launch_bounds__(kShadeBlock) cluster_shade_kernel(DevScene s, const rzk_receiver *recv,
+                                                                    SliceTables t, VisTables v, int mode, float tau,
+                                                                    float *sums) {
+    const int item = (int)(((long long)blockIdx.x * kShadeBlock + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (item >= t.n_items) return;
+    int lo = 0, hi = t.n_slices - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (t.tile_off[mid] <= item) lo = mid; else hi = mid - 1;
+    }
+    const int sl = t.order[lo];
+    const int wt = item - t.tile_off[lo];
+    const int po = t.pix_off[sl], nr = t.pix_cnt[sl], ro = t.rep_off[sl], nc = t.rep_cnt[sl];
+    shade_item<true>(s, recv + po, nr, t.reps + ro, nc, v.masks + v.mask_off[lo] + (long long)wt * nc, wt, mode,
+                     tau, sums + 3 * (size_t)po, lane, t.weights + ro);
 }
 
 __global__ void scatter_kernel(const float *sums, const int *pix, int n, float scale, float *out) {
@@ -635,7 +672,9 @@ struct rzk_lightslice {
     DBuf<float> g_box, g_rep, g_uvn, g_prob, g_row_cdf, g_col_cdf, g_total;
     DBuf<uint8_t> g_valid;
     // per-gather scratch (grown on demand)
-    DBuf<int> d_slice, d_count, d_off, d_cursor, d_pix, d_tile_off, d_work;
+    DBuf<int> d_slice, d_count, d_off, d_cursor, d_pix, d_tile_off, d_order, d_vis_off, d_work;
+    DBuf<long long> d_mask_off;
+    DBuf<uint32_t> d_masks;   // visibility ballots of the tracing pass
     DBuf<uint32_t> d_keys;
     DBuf<unsigned char> d_sort;
     DBuf<rzk_receiver> d_perm;
@@ -1045,7 +1084,7 @@ int cluster_gather_grid() {
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cluster_gather_kernel<4, 32, 5>, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cluster_vis_kernel<4, 32, 5>, 128, 0);
     return std::max(1, sms * std::max(1, per_sm));
 }
 
@@ -1306,6 +1345,9 @@ rzk_status rzk_lightslice_gather(rzk_lightslice *L, const rzk_receiver *d_recv, 
         LS_TRY(L->d_off.alloc(ns + 1));
         LS_TRY(L->d_cursor.alloc(ns + 1));
         LS_TRY(L->d_tile_off.alloc(ns + 1));
+        LS_TRY(L->d_order.alloc(ns + 1));
+        LS_TRY(L->d_vis_off.alloc(ns + 1));
+        LS_TRY(L->d_mask_off.alloc(ns + 1));
         LS_TRY(L->d_work.alloc(1));
     }
     // slice of every pixel and the bin sizes
@@ -1316,16 +1358,37 @@ rzk_status rzk_lightslice_gather(rzk_lightslice *L, const rzk_receiver *d_recv, 
     std::vector<int> cnt(ns);
     LS_TRY(cudaMemcpyAsync(cnt.data(), L->d_count.p, sizeof(int) * ns, cudaMemcpyDeviceToHost, st));
     LS_TRY(cudaStreamSynchronize(st));
-    std::vector<int> off(ns + 1), toff(ns + 1);
+    std::vector<int> off(ns + 1), toff(ns + 1), order(ns);
     off[0] = 0;
+    for (int s = 0; s < ns; ++s) off[s + 1] = off[s] + cnt[s];
+    // Work items are handed out in order of decreasing cost: the tiles of the slices with
+    // the most representatives first (a tile costs its 32 pixels x the slice's
+    // representatives), so that the last items to start are short ones.  Every pixel still
+    // adds its slice's representatives in cluster order; only which warp takes which tile,
+    // and when, changes.
+    for (int s = 0; s < ns; ++s) order[s] = s;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return L->clusters[a].size() > L->clusters[b].size(); });
     toff[0] = 0;
-    for (int s = 0; s < ns; ++s) {
-        off[s + 1] = off[s] + cnt[s];
-        toff[s + 1] = toff[s] + (cnt[s] + 31) / 32;
+    for (int p = 0; p < ns; ++p) toff[p + 1] = toff[p] + (cnt[order[p]] + 31) / 32;
+    std::vector<int> voff(ns + 1);
+    std::vector<long long> moff(ns + 1);
+    voff[0] = 0;
+    moff[0] = 0;
+    for (int p = 0; p < ns; ++p) {
+        const long long tiles = (cnt[order[p]] + 31) / 32, nc = (long long)L->clusters[order[p]].size();
+        const long long items = voff[p] + tiles * ((nc + kVisChunk - 1) / kVisChunk);
+        if (items >= (1LL << 31)) return RZK_ERR_CAPACITY;
+        voff[p + 1] = (int)items;
+        moff[p + 1] = moff[p] + tiles * nc;
     }
+    if ((size_t)moff[ns] > L->d_masks.n) LS_TRY(L->d_masks.alloc((size_t)moff[ns]));
     const int binned = off[ns];
     LS_TRY(cudaMemcpyAsync(L->d_off.p, off.data(), sizeof(int) * (ns + 1), cudaMemcpyHostToDevice, st));
     LS_TRY(cudaMemcpyAsync(L->d_tile_off.p, toff.data(), sizeof(int) * (ns + 1), cudaMemcpyHostToDevice, st));
+    LS_TRY(cudaMemcpyAsync(L->d_order.p, order.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, st));
+    LS_TRY(cudaMemcpyAsync(L->d_vis_off.p, voff.data(), sizeof(int) * (ns + 1), cudaMemcpyHostToDevice, st));
+    LS_TRY(cudaMemcpyAsync(L->d_mask_off.p, moff.data(), sizeof(long long) * (ns + 1), cudaMemcpyHostToDevice, st));
     // bins: a stable sort of the pixels by (slice, Morton code) - see bin_keys_kernel
     int sbits = 1;
     while ((1 << sbits) < ns + 1) ++sbits;
@@ -1349,6 +1412,7 @@ rzk_status rzk_lightslice_gather(rzk_lightslice *L, const rzk_receiver *d_recv, 
         gather_recv_kernel<<<(binned + 255) / 256, 256, 0, st>>>(d_recv, L->d_pix.p, binned, L->d_perm.p);
         SliceTables t;
         t.tile_off = L->d_tile_off.p;
+        t.order = L->d_order.p;
         t.pix_off = L->d_off.p;
         t.pix_cnt = L->d_count.p;
         t.rep_off = L->d_rep_off.p;
@@ -1357,11 +1421,21 @@ rzk_status rzk_lightslice_gather(rzk_lightslice *L, const rzk_receiver *d_recv, 
         t.weights = L->d_weights.p;
         t.n_slices = ns;
         t.n_items = toff[ns];
+        VisTables v;
+        v.vis_off = L->d_vis_off.p;
+        v.mask_off = L->d_mask_off.p;
+        v.masks = L->d_masks.p;
+        v.n_items = voff[ns];
         LS_TRY(cudaMemsetAsync(L->d_work.p, 0, sizeof(int), st));
         static int grid = 0;   // resident grid of the persistent kernel (one device per process)
         if (grid == 0) grid = cluster_gather_grid();
-        cluster_gather_kernel<4, 32, 5><<<grid, 128, 0, st>>>(L->scene->dev(), L->d_perm.p, t, clamp_mode, tau,
-                                                              L->d_sums.p, L->d_work.p);
+        const DevScene ds = L->scene->dev();
+        if (v.n_items > 0)
+            cluster_vis_kernel<4, 32, 5><<<grid, 128, 0, st>>>(ds, L->d_perm.p, t, v, L->d_work.p);
+        LS_TRY(cudaGetLastError());
+        const long long threads = 32LL * t.n_items;
+        cluster_shade_kernel<<<(unsigned)((threads + kShadeBlock - 1) / kShadeBlock), kShadeBlock, 0, st>>>(
+            ds, L->d_perm.p, t, v, clamp_mode, tau, L->d_sums.p);
         LS_TRY(cudaGetLastError());
         scatter_kernel<<<(binned + 255) / 256, 256, 0, st>>>(L->d_sums.p, L->d_pix.p, binned, scale, d_rgb);
         LS_TRY(cudaGetLastError());
