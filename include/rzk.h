@@ -324,7 +324,9 @@ rzk_status rzk_mrcs_clusters(const rzk_mrcs *mrcs, int32_t *h_pixels, int32_t *h
 /* MatrixRowColumnSampling::gather_clusters (mrcs.cc:28-41) for every receiver:
  * d_rgb[r] = scale * sum over clusters of weight x radiance(r, representative), added in
  * cluster order (the integrator divides by num_emitted_photons, vpl.cc:481-484: pass
- * scale = 1 / num_emitted).  image_width as in rzk_gather_cfg. */
+ * scale = 1 / num_emitted).  image_width as in rzk_gather_cfg.  Runs as a tracing pass
+ * (visibility ballots, one 32-bit word per warp tile and representative, held by the
+ * object and grown by the first gather of a larger image) and a summing pass. */
 rzk_status rzk_mrcs_gather(rzk_mrcs *mrcs, const rzk_receiver *d_recv, int n_recv, int image_width,
                            float scale, float *d_rgb, void *stream);
 

@@ -331,15 +331,15 @@ __device__ __forceinline__ bool gather_item(const DevScene &s, const rzk_receive
 }
 
 // Visibility half of gather_item, for gathers split into a tracing pass and a summing
-// pass: the 32 receivers of warp tile `wt` against VPLs [j0, j1); masks[j - j0] = ballot of
+// pass: the 32 receivers of warp tile `wt` (img_w as in lane_receiver) against VPLs [j0, j1); masks[j - j0] = ballot of
 // the lanes whose pair's term is not exactly zero (pair_survives) and whose shadow segment
 // is unoccluded - exactly the pairs gather_item adds.  Returns false if a bounded wait gave
 // up (reported in the error word).
 template <int TILE>
-__device__ __forceinline__ bool visibility_item(const DevScene &s, const rzk_receiver *recv, int n_recv,
+__device__ __forceinline__ bool visibility_item(const DevScene &s, const rzk_receiver *recv, int n_recv, int img_w,
                                                 const rzk_vpl *vpls, int j0, int j1, int wt, WarpStage<TILE> &ws,
                                                 int lane, uint32_t *masks) {
-    const int ri = lane_receiver(wt, lane, n_recv, 0);
+    const int ri = lane_receiver(wt, lane, n_recv, img_w);
     const int n_tiles = (j1 - j0 + TILE - 1) / TILE;
     RecvRegs r;
     r.p = mk(0.0f, 0.0f, 0.0f);
@@ -395,10 +395,10 @@ __device__ __forceinline__ bool visibility_item(const DevScene &s, const rzk_rec
 // the same order as gather_item with one chunk, so the sums are bit-identical to it.
 // WEIGHTED as in gather_item.  Writes partial[3 * ri ...].
 template <bool WEIGHTED>
-__device__ __forceinline__ void shade_item(const DevScene &s, const rzk_receiver *recv, int n_recv,
+__device__ __forceinline__ void shade_item(const DevScene &s, const rzk_receiver *recv, int n_recv, int img_w,
                                            const rzk_vpl *vpls, int n_vpl, const uint32_t *masks, int wt, int mode,
                                            float tau, float *partial, int lane, const float *weights) {
-    const int ri = lane_receiver(wt, lane, n_recv, 0);
+    const int ri = lane_receiver(wt, lane, n_recv, img_w);
     if (ri < 0) return;
     RecvRegs r = load_receiver(recv + ri);
     Rgb sum = crgb(0.0f, 0.0f, 0.0f);

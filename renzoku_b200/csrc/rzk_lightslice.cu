@@ -196,7 +196,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) cluster_vis_kernel(DevScene 
         const int j0 = c * kVisChunk, j1 = min(nc, j0 + kVisChunk);
         const int po = t.pix_off[sl], nr = t.pix_cnt[sl], ro = t.rep_off[sl];
         uint32_t *m = v.masks + v.mask_off[lo] + (long long)wt * nc + j0;
-        if (!visibility_item<TILE>(s, recv + po, nr, t.reps + ro, j0, j1, wt, ws, lane, m)) break;
+        if (!visibility_item<TILE>(s, recv + po, nr, 0, t.reps + ro, j0, j1, wt, ws, lane, m)) break;
     }
 }
 
@@ -215,7 +215,7 @@ __global__ void __launch_bounds__(kShadeBlock) cluster_shade_kernel(DevScene s, 
     const int sl = t.order[lo];
     const int wt = item - t.tile_off[lo];
     const int po = t.pix_off[sl], nr = t.pix_cnt[sl], ro = t.rep_off[sl], nc = t.rep_cnt[sl];
-    shade_item<true>(s, recv + po, nr, t.reps + ro, nc, v.masks + v.mask_off[lo] + (long long)wt * nc, wt, mode,
+    shade_item<true>(s, recv + po, nr, 0, t.reps + ro, nc, v.masks + v.mask_off[lo] + (long long)wt * nc, wt, mode,
                      tau, sums + 3 * (size_t)po, lane, t.weights + ro);
 }
 

@@ -14,8 +14,8 @@
 //   4. ClusterBuilder::cluster_by_sampling on it (device distances, host draws that
 //      continue the same stream).
 // Gathering (rzk_mrcs_gather, MatrixRowColumnSampling::gather_clusters, mrcs.cc:28-41):
-// per receiver, the weighted sum over the clusters' representatives in cluster order -
-// the persistent warp-packet gather with the representatives as one weighted VPL chunk.
+// per receiver, the weighted sum over the clusters' representatives in cluster order - a
+// tracing pass of warp-packet visibility ballots, then an in-order summing pass.
 #include "rzk_gather_dev.cuh"
 #include "rzk_cluster.cuh"
 #include "rzk_hostutil.h"
@@ -58,30 +58,50 @@ __global__ void take_reps_kernel(const rzk_vpl *vpls, const int *rep, int n, rzk
     reinterpret_cast<uint32_t *>(out)[w] = reinterpret_cast<const uint32_t *>(vpls + rep[c])[i];
 }
 
-// gather_clusters for every receiver: warp tiles from an atomic counter, the
-// representatives streamed as one weighted chunk, so each receiver adds
-// weight x radiance in cluster order (mrcs.cc:31-39).
+// gather_clusters for every receiver, in two passes so that the work splits finely
+// without changing any sum.  Tracing: items (warp tile, run of kVisChunk representatives)
+// from an atomic counter, each storing one visibility ballot per representative.  Summing:
+// one warp per tile adds weight x radiance over the representatives in cluster order for
+// the pairs the ballots mark - the pairs and the order of a one-pass gather
+// (mrcs.cc:31-39).
+constexpr int kVisChunk = 128;
+
 template <int WARPS, int TILE, int MINB>
-__global__ void __launch_bounds__(WARPS * 32, MINB) mrcs_gather_kernel(DevScene s, const rzk_receiver *recv,
-                                                                       int n_recv, int img_w, const rzk_vpl *reps,
-                                                                       const float *weights, int n_reps,
-                                                                       int n_wtiles, int *work, int mode, float tau,
-                                                                       float *sums) {
+__global__ void __launch_bounds__(WARPS * 32, MINB) mrcs_vis_kernel(DevScene s, const rzk_receiver *recv,
+                                                                    int n_recv, int img_w, const rzk_vpl *reps,
+                                                                    int n_reps, int n_wtiles, int *work,
+                                                                    uint32_t *masks) {
     __shared__ __align__(128) rzk_vpl tiles[WARPS][2][TILE];
     __shared__ __align__(8) uint64_t bar[WARPS][2];
     __shared__ int stacks[WARPS][STACK_CAP];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     WarpStage<TILE> ws;
     ws.init(tiles[w], bar[w], stacks[w], lane);
+    const int nch = (n_reps + kVisChunk - 1) / kVisChunk;
+    const long long n_items = (long long)n_wtiles * nch;
     while (true) {
         int item = 0;
         if (lane == 0) item = atomicAdd(work, 1);
         item = __shfl_sync(kFull, item, 0);
-        if (item >= n_wtiles) break;
-        if (!gather_item<TILE, true>(s, recv, n_recv, img_w, reps, n_reps, 0, item, n_reps, mode, tau, sums, ws,
-                                     lane, weights))
+        if (item >= n_items) break;
+        const int wt = item / nch, c = item - wt * nch;
+        const int j0 = c * kVisChunk, j1 = min(n_reps, j0 + kVisChunk);
+        if (!visibility_item<TILE>(s, recv, n_recv, img_w, reps, j0, j1, wt, ws, lane,
+                                   masks + (long long)wt * n_reps + j0))
             break;
     }
+}
+
+constexpr int kShadeBlock = 128;
+
+__global__ void __launch_bounds__(kShadeBlock) mrcs_shade_kernel(DevScene s, const rzk_receiver *recv, int n_recv,
+                                                                 int img_w, const rzk_vpl *reps, const float *weights,
+                                                                 int n_reps, int n_wtiles, const uint32_t *masks,
+                                                                 int mode, float tau, float *sums) {
+    const int wt = (int)(((long long)blockIdx.x * kShadeBlock + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (wt >= n_wtiles) return;
+    shade_item<true>(s, recv, n_recv, img_w, reps, n_reps, masks + (long long)wt * n_reps, wt, mode, tau, sums,
+                     lane, weights);
 }
 
 __global__ void scale_kernel(float *x, long long n, float scale) {
@@ -121,6 +141,8 @@ struct rzk_mrcs {
     rzk::DBuf<float> weights;
     int weight_n = 0;                            // clusters with a representative
     rzk::DBuf<int> work;
+    rzk::DBuf<uint32_t> masks;                   // visibility ballots of the tracing pass
+    size_t mask_words = 0;
     int grid = 0;
     float ms[4] = {0, 0, 0, 0};
 };
@@ -297,7 +319,7 @@ rzk_status rzk_mrcs_create(rzk_context *ctx, rzk_scene *scene, const rzk_camera 
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mrcs_gather_kernel<4, 32, 5>, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mrcs_vis_kernel<4, 32, 5>, 128, 0);
     m->grid = std::max(1, sms * std::max(1, per_sm));
     *out = m;
     return RZK_OK;
@@ -338,11 +360,25 @@ rzk_status rzk_mrcs_gather(rzk_mrcs *m, const rzk_receiver *d_recv, int n_recv, 
     } else {
         wtiles = ((long long)n_recv + 31) / 32;
     }
-    if (wtiles >= (1LL << 31)) return RZK_ERR_CAPACITY;
-    RZK_CUDA_TRY(cudaMemsetAsync(m->work.p, 0, sizeof(int), st));
-    mrcs_gather_kernel<4, 32, 5><<<m->grid, 128, 0, st>>>(m->scene->dev(), d_recv, n_recv, image_width, m->reps.p,
-                                                          m->weights.p, m->weight_n, (int)wtiles, m->work.p,
-                                                          m->clamp_mode, m->tau, d_rgb);
+    const int nr = m->weight_n;
+    const long long nch = (nr + kVisChunk - 1) / kVisChunk;
+    if (wtiles * std::max<long long>(nch, 1) >= (1LL << 31)) return RZK_ERR_CAPACITY;
+    const size_t words = (size_t)wtiles * (size_t)nr;
+    if (words > m->mask_words) {   // grows with the image: the first gather of a size allocates
+        RZK_CUDA_TRY(m->masks.alloc(words));
+        m->mask_words = words;
+    }
+    const DevScene ds = m->scene->dev();
+    if (nr > 0) {
+        RZK_CUDA_TRY(cudaMemsetAsync(m->work.p, 0, sizeof(int), st));
+        mrcs_vis_kernel<4, 32, 5><<<m->grid, 128, 0, st>>>(ds, d_recv, n_recv, image_width, m->reps.p, nr,
+                                                           (int)wtiles, m->work.p, m->masks.p);
+        RZK_CUDA_TRY(cudaGetLastError());
+    }
+    const long long threads = 32LL * wtiles;
+    mrcs_shade_kernel<<<(unsigned)((threads + kShadeBlock - 1) / kShadeBlock), kShadeBlock, 0, st>>>(
+        ds, d_recv, n_recv, image_width, m->reps.p, m->weights.p, nr, (int)wtiles, m->masks.p, m->clamp_mode,
+        m->tau, d_rgb);
     RZK_CUDA_TRY(cudaGetLastError());
     const long long n3 = 3LL * n_recv;
     scale_kernel<<<(unsigned)((n3 + 255) / 256), 256, 0, st>>>(d_rgb, n3, scale);
