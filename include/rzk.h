@@ -99,6 +99,48 @@ rzk_status rzk_primary(rzk_scene *scene, const rzk_camera *h_cam, rzk_receiver *
 rzk_status rzk_camera_setup(const float eye[3], const float lookat[3], const float up[3],
                             float fov_deg, int width, int height, float film_w, float film_h,
                             rzk_camera *h_out);
+/* The same from a focal length: Camera::set_perspective(eye, lookat, up, focal, sensor)
+ * (camera.cc:23-30), as the OBJ importer's camera line gives it (obj_importer.cc:236-246). */
+rzk_status rzk_camera_setup_focal(const float eye[3], const float lookat[3], const float up[3],
+                                  float focal, int width, int height, float film_w, float film_h,
+                                  rzk_camera *h_out);
+
+/* OBJ / MTL scenes --------------------------------------------------------------------- */
+
+/* A Wavefront OBJ scene in the reference's dialect, imported on the host: the reference
+ * parser (obj_parser.cpp) and ObjImporter::load (obj_importer.cc:212-553), giving the
+ * same surfaces in the same order (light quads, then faces in file order) with the same
+ * BSDF parameters and light radiances.  What this path does not model is counted in
+ * rzk_obj_info and left out; the scene equals the reference's where those counts are 0. */
+typedef struct rzk_obj rzk_obj;
+typedef struct {
+    int32_t n_prims, n_mats, n_lights;   /* the scene description's primitives, materials,
+                                            area lights */
+    int32_t has_camera;                  /* the first `c` line: Camera::set_perspective(eye,
+                                            lookat, up, focal) on a 512 x 512 sensor with a
+                                            0.025 x 0.025 film (obj_importer.cc:234-252) */
+    float eye[3], lookat[3], up[3], focal;
+    int32_t width, height;
+    float film_w, film_h;
+    int32_t point_lights;                /* `lp` lines: point lights, not imported */
+    int32_t spheres;                     /* `sp` lines: analytic spheres, not imported */
+    int32_t faces_without_material;      /* no surface in the reference either */
+    int32_t faces_unsupported_material;  /* refractive (Ni > 1) or textured (map_Kd): left out */
+    int32_t short_faces;                 /* fewer than 3 vertices: skipped by the reference too */
+    int32_t faces_with_vertex_normals;   /* imported with facet normals (the reference
+                                            interpolates the given normals) */
+    int32_t smoothed_faces;              /* smoothing group > 0: facet normals here */
+    int32_t mtl_files_missing;           /* mtllib files that could not be read */
+} rzk_obj_info;
+
+/* Reads `path` (and its mtllib files, relative to its directory).  RZK_ERR_INVALID when the
+ * file cannot be read or an index points outside its lists. */
+rzk_status rzk_obj_import(const char *path, rzk_obj **out);
+rzk_status rzk_obj_get_info(const rzk_obj *obj, rzk_obj_info *info);
+/* Fills `desc` with pointers into the object (valid until rzk_obj_destroy), ready for
+ * rzk_scene_create; tmin is the reference's RAY_TMIN. */
+rzk_status rzk_obj_scene_desc(const rzk_obj *obj, rzk_scene_desc *desc);
+rzk_status rzk_obj_destroy(rzk_obj *obj);
 
 /* Warm restart: a built scene as one host blob (device arrays and host-side counts), and
  * back.  No reference counterpart (the reference rebuilds its BVH from the scene file on

@@ -279,6 +279,8 @@ class RefHarness:
             L.rref_ls_gather.argtypes = [P, P, I32, I32, F32, P]
             L.rref_ls_guided.argtypes = [P, P, I32, I32, I32, I32, F32, I32, U32, P]
             L.rref_matrix_save.argtypes = [P, I32, I32, ctypes.c_char_p]
+            L.rref_obj_import.restype = I32
+            L.rref_obj_import.argtypes = [ctypes.c_char_p, I32, P, P, P, P, P, P, P, P, P, P, P]
             L.rref_mrcs.restype = I32
             L.rref_mrcs.argtypes = [P, P, I32, I32, F32, U32, I32, F32, I32, P, I32, P, P, P, P, I32]
             cls._lib = L
@@ -374,6 +376,24 @@ class RefHarness:
         n = self.lib().rref_cluster_by_sampling(self.h, _ptr(mat), rows, cols, num_clusters, seed,
                                                 _ptr(c), _ptr(r), _ptr(w), _ptr(a))
         return c[:n], r[:n], w[:n], a
+
+    @classmethod
+    def obj_import(cls, path, cap=100000):
+        """The reference's ObjImporter::load on `path`: per triangle / quad surface in order,
+        (kind, vertices [12], is_light, radiance, Bsdf::Type or -1, kd, ks, glossy [2]), the
+        camera record (or None) and the total surface count."""
+        kind = np.zeros(cap, np.int32); v = np.zeros((cap, 12), np.float32)
+        light = np.zeros(cap, np.int32); emit = np.zeros((cap, 3), np.float32)
+        mtype = np.zeros(cap, np.int32); kd = np.zeros((cap, 3), np.float32)
+        ks = np.zeros((cap, 3), np.float32); gl = np.zeros((cap, 2), np.float32)
+        cam = np.zeros(1, sg.CAMERA_DTYPE)
+        has_cam, n_surf = ctypes.c_int32(), ctypes.c_int32()
+        k = cls.lib().rref_obj_import(str(path).encode(), cap, _ptr(kind), _ptr(v), _ptr(light), _ptr(emit),
+                                      _ptr(mtype), _ptr(kd), _ptr(ks), _ptr(gl), _ptr(cam),
+                                      ctypes.byref(has_cam), ctypes.byref(n_surf))
+        out = {"kind": kind[:k], "v": v[:k], "light": light[:k], "emit": emit[:k], "type": mtype[:k],
+               "kd": kd[:k], "ks": ks[:k], "glossy": gl[:k]}
+        return out, (cam if has_cam.value else None), n_surf.value
 
     @classmethod
     def matrix_save(cls, mat, path):

@@ -275,11 +275,16 @@ rzk_status rzk_primary(rzk_scene *s, const rzk_camera *cam, rzk_receiver *d_out,
 
 rzk_status rzk_camera_setup(const float eye[3], const float lookat[3], const float up[3], float fov_deg,
                             int width, int height, float film_w, float film_h, rzk_camera *o) {
-    if (!eye || !lookat || !up || !o || width <= 0 || height <= 0) return RZK_ERR_INVALID;
-    memset(o, 0, sizeof(*o));
     const float DEGREE_TO_RADIAN = A_PI / 180.0f;
     // Camera::focal_length_from_fov (camera.h:228-230)
     float focal = film_h / (2.0f * tanf(fov_deg / 2 * DEGREE_TO_RADIAN));
+    return rzk_camera_setup_focal(eye, lookat, up, focal, width, height, film_w, film_h, o);
+}
+
+rzk_status rzk_camera_setup_focal(const float eye[3], const float lookat[3], const float up[3], float focal,
+                                  int width, int height, float film_w, float film_h, rzk_camera *o) {
+    if (!eye || !lookat || !up || !o || width <= 0 || height <= 0) return RZK_ERR_INVALID;
+    memset(o, 0, sizeof(*o));
     V3 e = ld3(eye), l = ld3(lookat), u = ld3(up);
     // Onb::init_from_nv(eye - lookat, up) (camera.cc:25, onb.cc:117-127)
     V3 nn = sub(e, l);

@@ -59,6 +59,11 @@ SIGNATURES = [
     ("rzk_closest_batch", I32, [P, P, P, I32, P, P, P]),
     ("rzk_primary", I32, [P, P, P, P]),
     ("rzk_camera_setup", I32, [P, P, P, F32, I32, I32, F32, F32, P]),
+    ("rzk_camera_setup_focal", I32, [P, P, P, F32, I32, I32, F32, F32, P]),
+    ("rzk_obj_import", I32, [ctypes.c_char_p, P]),
+    ("rzk_obj_get_info", I32, [P, P]),
+    ("rzk_obj_scene_desc", I32, [P, P]),
+    ("rzk_obj_destroy", I32, [P]),
     ("rzk_vpl_generate", I32, [P, U32, I32, I32, P, I32, P, P]),
     ("rzk_gather", I32, [P, P, P, I32, P, I32, I32, F32, F32, P, P]),
     ("rzk_gather_variants", I32, []),
@@ -200,6 +205,19 @@ class Camera:
                                    spec.width, spec.height, spec.film_w, spec.film_h,
                                    self.rec.ctypes.data), "rzk_camera_setup")
 
+    @classmethod
+    def from_focal(cls, eye, lookat, up, focal: float, width: int, height: int, film_w: float,
+                   film_h: float) -> "Camera":
+        """Camera::set_perspective with a focal length (the OBJ camera line)."""
+        self = cls.__new__(cls)
+        self.spec = sg.CameraSpec(tuple(eye), tuple(lookat), tuple(up), float("nan"), width, height, film_w, film_h)
+        self.rec = np.zeros(1, sg.CAMERA_DTYPE)
+        f = lambda t: np.asarray(t, np.float32)
+        e, l, u = f(eye), f(lookat), f(up)
+        check(load().rzk_camera_setup_focal(e.ctypes.data, l.ctypes.data, u.ctypes.data, focal, width, height,
+                                            film_w, film_h, self.rec.ctypes.data), "rzk_camera_setup_focal")
+        return self
+
     @property
     def n_pixels(self) -> int:
         return self.spec.width * self.spec.height
@@ -211,6 +229,48 @@ class Camera:
     @property
     def height(self) -> int:
         return self.spec.height
+
+
+class ObjInfoC(ctypes.Structure):
+    """ctypes mirror of rzk_obj_info."""
+    _fields_ = [("n_prims", I32), ("n_mats", I32), ("n_lights", I32), ("has_camera", I32),
+                ("eye", F32 * 3), ("lookat", F32 * 3), ("up", F32 * 3), ("focal", F32),
+                ("width", I32), ("height", I32), ("film_w", F32), ("film_h", F32),
+                ("point_lights", I32), ("spheres", I32), ("faces_without_material", I32),
+                ("faces_unsupported_material", I32), ("short_faces", I32),
+                ("faces_with_vertex_normals", I32), ("smoothed_faces", I32), ("mtl_files_missing", I32)]
+
+
+def import_obj(path: str):
+    """A Wavefront OBJ scene in the reference's dialect (rzk_obj_import): returns
+    (scenegen.Scene, Camera or None, info dict of what was counted and left out)."""
+    lib = load()
+    h = ctypes.c_void_p()
+    check(lib.rzk_obj_import(str(path).encode(), ctypes.byref(h)), "rzk_obj_import")
+    try:
+        info = ObjInfoC()
+        check(lib.rzk_obj_get_info(h, ctypes.byref(info)), "rzk_obj_get_info")
+        d = sg.SceneDescC()
+        check(lib.rzk_obj_scene_desc(h, ctypes.byref(d)), "rzk_obj_scene_desc")
+        n, m = d.n_prims, d.n_mats
+
+        def arr(ptr, dtype, count):
+            if count == 0:
+                return np.zeros(0, dtype)
+            return np.frombuffer(ctypes.string_at(ptr, np.dtype(dtype).itemsize * count), dtype).copy()
+
+        spec = sg.CameraSpec(tuple(info.eye), tuple(info.lookat), tuple(info.up), float("nan"), info.width,
+                             info.height, info.film_w, info.film_h)
+        scene = sg.Scene(os.path.splitext(os.path.basename(str(path)))[0], arr(d.prim_kind, np.int32, n),
+                         arr(d.prim_v, np.float32, 12 * n).reshape(n, 12), arr(d.prim_mat, np.int32, n),
+                         arr(d.prim_emit, np.float32, 3 * n).reshape(n, 3), arr(d.prim_flags, np.int32, n),
+                         arr(d.mats, sg.MATERIAL_DTYPE, m), spec, d.tmin)
+        cam = (Camera.from_focal(info.eye, info.lookat, info.up, info.focal, info.width, info.height,
+                                 info.film_w, info.film_h) if info.has_camera else None)
+        out = {k: getattr(info, k) for k, _ in ObjInfoC._fields_ if k not in ("eye", "lookat", "up")}
+        return scene, cam, out
+    finally:
+        lib.rzk_obj_destroy(h)
 
 
 class AggregateCuda:
