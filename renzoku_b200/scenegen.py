@@ -331,3 +331,41 @@ def room_filled(n_tris_target: int, width: int, height: int, seed: int) -> Scene
                      seed_mat=seed + 1)
     s.name = f"room_filled_{n_tris_target}"
     return s
+
+
+def write_obj(scene: Scene, path: str) -> None:
+    """Writes `scene` as an OBJ file and its MTL file (same name, .mtl) in the reference's
+    OBJ dialect (obj_parser.cpp, obj_importer.cc), which rzk_obj_import reads back: every
+    primitive as a face of its own vertices, materials as `mat_<i>` (Lambertian: Kd;
+    Phong: Kd, Ks, Ns n; Ward: Kd, Ks, Ns 1/ax 1/ay), each emitter with a material
+    `rz_light_<k>` whose Kd is its radiance.  Reals are written with 9 significant digits,
+    so float32 values read back unchanged.  The format has no surface flags: surfaces read
+    back one-sided, as the reference's importer builds them."""
+    import os
+    base = os.path.splitext(path)[0]
+    mtl_path = base + ".mtl"
+    g = lambda x: "%.9g" % float(x)
+    with open(mtl_path, "w") as f:
+        for i, m in enumerate(scene.mats):
+            f.write(f"newmtl mat_{i}\n")
+            f.write("Kd " + " ".join(g(x) for x in m["kd"]) + "\n")
+            if int(m["type"]) == BSDF_PHONG:
+                f.write("Ks " + " ".join(g(x) for x in m["ks"]) + "\n")
+                f.write(f"Ns {g(m['p0'])}\n")
+            elif int(m["type"]) == BSDF_WARD:
+                f.write("Ks " + " ".join(g(x) for x in m["ks"]) + "\n")
+                f.write(f"Ns {g(np.float32(1.0) / m['p0'])} {g(np.float32(1.0) / m['p1'])}\n")
+        lights = np.nonzero(scene.prim_mat < 0)[0]
+        for k, p in enumerate(lights):
+            f.write(f"newmtl rz_light_{k}\n")
+            f.write("Kd " + " ".join(g(x) for x in scene.prim_emit[p]) + "\n")
+    light_of = {int(p): k for k, p in enumerate(lights)}
+    with open(path, "w") as f:
+        f.write(f"mtllib {os.path.basename(mtl_path)}\n")
+        for p in range(scene.n_prims):
+            n = int(scene.prim_kind[p])
+            for j in range(n):
+                f.write("v " + " ".join(g(x) for x in scene.prim_v[p, 3 * j:3 * j + 3]) + "\n")
+            name = f"rz_light_{light_of[p]}" if scene.prim_mat[p] < 0 else f"mat_{int(scene.prim_mat[p])}"
+            f.write(f"usemtl {name}\n")
+            f.write("f " + " ".join(str(-n + j) for j in range(n)) + "\n")
