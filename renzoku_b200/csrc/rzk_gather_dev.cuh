@@ -253,13 +253,11 @@ struct WarpStage {
 
 // One work item of the persistent gather: the 32 receivers of warp tile `wt` against VPL
 // chunk `chunk`; writes that chunk's partial sums.  Returns false if a bounded wait gave
-// up (reported in the error word).  WEIGHTED: VPL j's radiance is multiplied by
-// weights[j] before it is added (a cluster representative standing for its cluster).
-template <int TILE, bool WEIGHTED = false>
+// up (reported in the error word).
+template <int TILE>
 __device__ __forceinline__ bool gather_item(const DevScene &s, const rzk_receiver *recv, int n_recv, int img_w,
                                             const rzk_vpl *vpls, int n_vpl, int chunk, int wt, int chunk_len,
-                                            int mode, float tau, float *partial, WarpStage<TILE> &ws,
-                                            int lane, const float *weights = nullptr) {
+                                            int mode, float tau, float *partial, WarpStage<TILE> &ws, int lane) {
     const int ri = lane_receiver(wt, lane, n_recv, img_w);
     const int j0 = chunk * chunk_len;
     const int j1 = min(n_vpl, j0 + chunk_len);
@@ -313,12 +311,7 @@ __device__ __forceinline__ bool gather_item(const DevScene &s, const rzk_receive
             Ray ray = make_ray(r.p, sub(pg.q, r.p));
             float tmax = len(sub(pg.q, r.p)) - s.tmin;
             if (packet_visible_near(s, ray, tmax, act, ws.stk, occ_cache)) {
-                Rgb L = pair_radiance(s, r, rm, l, pg, mode, tau);
-                if (WEIGHTED) {
-                    const float w = weights[j0 + k * TILE + v];
-                    L = crgb(w * L.r, w * L.g, w * L.b);
-                }
-                sum = cadd(sum, L);
+                sum = cadd(sum, pair_radiance(s, r, rm, l, pg, mode, tau));
             }
         }
         __syncwarp();
@@ -393,7 +386,8 @@ __device__ __forceinline__ bool visibility_item(const DevScene &s, const rzk_rec
 // Summing half: the 32 receivers of warp tile `wt` add, in VPL order, the terms of the
 // pairs that `masks` (one word per VPL, from visibility_item) marks - the same values in
 // the same order as gather_item with one chunk, so the sums are bit-identical to it.
-// WEIGHTED as in gather_item.  Writes partial[3 * ri ...].
+// WEIGHTED: VPL j's radiance is multiplied by weights[j] before it is added (a cluster
+// representative standing for its cluster).  Writes partial[3 * ri ...].
 template <bool WEIGHTED>
 __device__ __forceinline__ void shade_item(const DevScene &s, const rzk_receiver *recv, int n_recv, int img_w,
                                            const rzk_vpl *vpls, int n_vpl, const uint32_t *masks, int wt, int mode,
