@@ -146,9 +146,10 @@ __device__ __forceinline__ Rgb pair_radiance(const DevScene &s, const RecvRegs &
 // Packet any-hit, nearer child first by lane majority.  Returns whether this lane's
 // segment is unoccluded (lanes with act == false return false).
 // `cache` (per lane) names the any-hit-tree leaf whose triangle last occluded this lane's
-// receiver, or -1.  It is tried first: a triangle whose own box and triangle tests pass
-// occludes the segment whichever way it was found, so a hit there is the traversal's
-// answer; the leaf of any triangle the traversal finds replaces it.
+// receiver, or -1.  It is tried first, then the leaves cached by five neighbouring lanes: a
+// triangle whose own box and triangle tests pass occludes the segment whichever way it was
+// found, so a hit there is the traversal's answer; the leaf of any triangle found replaces
+// the lane's cache.
 __device__ __forceinline__ bool packet_visible_near(const DevScene &s, const Ray &ray, float tmax, bool act,
                                                     int *stk, int &cache) {
     if (s.n_nodes == 0) return act;
@@ -176,7 +177,30 @@ __device__ __forceinline__ bool packet_visible_near(const DevScene &s, const Ray
             if (tri_hit<false>(ta, tb, tc, ray, s.tmin, tmax, nullptr, nullptr, nullptr)) occluded = true;
         }
     }
-    // every lane takes part in the vote (the cache test above is per lane)
+    // Then the leaves cached by the lanes at xor distances 1, 8, 2, 16 and 4: in an 8 x 4
+    // pixel tile those are the neighbouring pixels, whose shadow rays toward the same VPL
+    // run almost parallel and are often blocked by the same triangle.  The same rule
+    // applies (own box and triangle tests), so the answer is still exact; a lane blocked by
+    // a neighbour's leaf adopts it.  Every lane takes part in each shuffle.
+    constexpr int kNeighbours[5] = {1, 8, 2, 16, 4};
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+        const int other = __shfl_xor_sync(kFull, cache, kNeighbours[q]);
+        if (alive && !occluded && other >= 0 && other != cache) {
+            const float4 *pc = s.trav + 2 * (other + 1);
+            const float4 c0 = __ldg(pc), c1 = __ldg(pc + 1);
+            float tc0 = 0.0f;
+            if (box_hit_fast(c0, c1, ray, s.tmin, tmax, tc0)) {
+                float4 ta, tb, tc;
+                load_tri(s, -1 - __float_as_int(c0.w), ta, tb, tc);
+                if (tri_hit<false>(ta, tb, tc, ray, s.tmin, tmax, nullptr, nullptr, nullptr)) {
+                    occluded = true;
+                    cache = other;
+                }
+            }
+        }
+    }
+    // every lane takes part in the vote (the cache tests above are per lane)
     alive = alive && !occluded;
     if (!__any_sync(kFull, alive)) return act && !occluded;
     // lanes whose root test failed cannot reach any triangle below it: they stay visible
