@@ -39,9 +39,9 @@ MAX_BOUNCE = 3
 TAU_PAIRS = 65536
 # DRAM bytes (read + write) of one full gather launch of this workload, from the one-pass
 # capture `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum -k regex:gather_persistent
-# -s 3 -c 1 python bench.py --steps 1 --warmup 3 --skip-cpu` (38.33 MB read, 56.27 MB
+# -s 3 -c 1 python bench.py --steps 1 --warmup 3 --skip-cpu` (37.58 MB read, 55.68 MB
 # written; the writes are the per-chunk partial sums), recorded in profiles/.
-TRAFFIC_BYTES_PER_LAUNCH = (38.32704 + 56.265472) * 1e6
+TRAFFIC_BYTES_PER_LAUNCH = (37.582336 + 55.679488) * 1e6
 
 
 def workload_config():
@@ -409,7 +409,7 @@ def run_ours(args):
                          "dram_gbs": dram_gbs, "dram_frac": None if dram_gbs is None else dram_gbs / peak,
                          "note": ("achieved counts the reference traversal's node and triangle bytes per "
                                   "evaluation (reference tree, reference visit order); the kernel visits fewer "
-                                  "nodes (SAH any-hit tree, occluder cache, Hilbert-ordered VPL chunks) and its "
+                                  "nodes (SAH any-hit tree, per-lane and neighbour occluder caches, Hilbert-ordered VPL chunks) and its "
                                   "~34 MB working set is L2-resident, so achieved exceeds the HBM copy peak; "
                                   "dram_gbs is the DRAM bandwidth the launch actually drew (traffic / duration)")},
             "cpu_baseline": {"value": cpu_v, "unit": "evals/s", "cores": threads, "kind": kind,
