@@ -145,13 +145,14 @@ __device__ __forceinline__ Rgb pair_radiance(const DevScene &s, const RecvRegs &
 
 // Packet any-hit, nearer child first by lane majority.  Returns whether this lane's
 // segment is unoccluded (lanes with act == false return false).
-// `cache` (per lane) names the any-hit-tree leaf whose triangle last occluded this lane's
-// receiver, or -1.  It is tried first, then the leaves cached by five neighbouring lanes: a
-// triangle whose own box and triangle tests pass occludes the segment whichever way it was
-// found, so a hit there is the traversal's answer; the leaf of any triangle found replaces
-// the lane's cache.
+// `cache` and `cache2` (per lane) name the any-hit-tree leaves whose triangles last
+// occluded this lane's receiver (most recent first), or -1.  They are tried first, then the
+// leaves cached by five neighbouring lanes: a triangle whose own box and triangle tests pass
+// occludes the segment whichever way it was found, so a hit there is the traversal's
+// answer; the leaf of any triangle found becomes the lane's `cache`, the previous one its
+// `cache2`.
 __device__ __forceinline__ bool packet_visible_near(const DevScene &s, const Ray &ray, float tmax, bool act,
-                                                    int *stk, int &cache) {
+                                                    int *stk, int &cache, int &cache2) {
     if (s.n_nodes == 0) return act;
     const float4 lo = __ldg(s.trav + 2), hi = __ldg(s.trav + 3);
     float t_root = 0.0f;
@@ -177,6 +178,21 @@ __device__ __forceinline__ bool packet_visible_near(const DevScene &s, const Ray
             if (tri_hit<false>(ta, tb, tc, ray, s.tmin, tmax, nullptr, nullptr, nullptr)) occluded = true;
         }
     }
+    if (alive && !occluded && cache2 >= 0 && cache2 != cache) {   // the one before it
+        const float4 *pc = s.trav + 2 * (cache2 + 1);
+        const float4 c0 = __ldg(pc), c1 = __ldg(pc + 1);
+        float tc0 = 0.0f;
+        if (box_hit_fast(c0, c1, ray, s.tmin, tmax, tc0)) {
+            float4 ta, tb, tc;
+            load_tri(s, -1 - __float_as_int(c0.w), ta, tb, tc);
+            if (tri_hit<false>(ta, tb, tc, ray, s.tmin, tmax, nullptr, nullptr, nullptr)) {
+                occluded = true;
+                const int t = cache;
+                cache = cache2;
+                cache2 = t;
+            }
+        }
+    }
     // Then the leaves cached by the lanes at xor distances 1, 8, 2, 16 and 4: in an 8 x 4
     // pixel tile those are the neighbouring pixels, whose shadow rays toward the same VPL
     // run almost parallel and are often blocked by the same triangle.  The same rule
@@ -195,6 +211,7 @@ __device__ __forceinline__ bool packet_visible_near(const DevScene &s, const Ray
                 load_tri(s, -1 - __float_as_int(c0.w), ta, tb, tc);
                 if (tri_hit<false>(ta, tb, tc, ray, s.tmin, tmax, nullptr, nullptr, nullptr)) {
                     occluded = true;
+                    cache2 = cache;
                     cache = other;
                 }
             }
@@ -220,7 +237,7 @@ __device__ __forceinline__ bool packet_visible_near(const DevScene &s, const Ray
             load_tri(s, -1 - al, ta, tb, tc);
             if (tri_hit<false>(ta, tb, tc, ray, s.tmin, tmax, nullptr, nullptr, nullptr)) {
                 occluded = true;
-                cache = c;
+                if (cache != c) { cache2 = cache; cache = c; }
             }
         }
         if (ar < 0 && hr && !occluded) {
@@ -228,7 +245,7 @@ __device__ __forceinline__ bool packet_visible_near(const DevScene &s, const Ray
             load_tri(s, -1 - ar, ta, tb, tc);
             if (tri_hit<false>(ta, tb, tc, ray, s.tmin, tmax, nullptr, nullptr, nullptr)) {
                 occluded = true;
-                cache = c + 1;
+                if (cache != c + 1) { cache2 = cache; cache = c + 1; }
             }
         }
         alive = alive && !occluded;
@@ -306,7 +323,7 @@ __device__ __forceinline__ bool gather_item(const DevScene &s, const rzk_receive
         return true;
     }
     Rgb sum = crgb(0.0f, 0.0f, 0.0f);
-    int occ_cache = -1;   // this lane's last occluder (any-hit tree leaf)
+    int occ_cache = -1, occ_cache2 = -1;   // this lane's last two occluders (any-hit tree leaves)
     if (lane == 0) {
         int cnt = min(TILE, j1 - j0);
         fence_proxy_async();
@@ -334,7 +351,7 @@ __device__ __forceinline__ bool gather_item(const DevScene &s, const rzk_receive
             if (!__any_sync(kFull, act)) continue;
             Ray ray = make_ray(r.p, sub(pg.q, r.p));
             float tmax = len(sub(pg.q, r.p)) - s.tmin;
-            if (packet_visible_near(s, ray, tmax, act, ws.stk, occ_cache)) {
+            if (packet_visible_near(s, ray, tmax, act, ws.stk, occ_cache, occ_cache2)) {
                 sum = cadd(sum, pair_radiance(s, r, rm, l, pg, mode, tau));
             }
         }
@@ -369,7 +386,7 @@ __device__ __forceinline__ bool visibility_item(const DevScene &s, const rzk_rec
         for (int j = j0 + lane; j < j1; j += 32) masks[j - j0] = 0u;
         return true;
     }
-    int occ_cache = -1;
+    int occ_cache = -1, occ_cache2 = -1;
     if (lane == 0) {
         int cnt = min(TILE, j1 - j0);
         fence_proxy_async();
@@ -398,7 +415,7 @@ __device__ __forceinline__ bool visibility_item(const DevScene &s, const rzk_rec
             if (__any_sync(kFull, act)) {
                 Ray ray = make_ray(r.p, sub(pg.q, r.p));
                 float tmax = len(sub(pg.q, r.p)) - s.tmin;
-                vis = __ballot_sync(kFull, packet_visible_near(s, ray, tmax, act, ws.stk, occ_cache));
+                vis = __ballot_sync(kFull, packet_visible_near(s, ray, tmax, act, ws.stk, occ_cache, occ_cache2));
             }
             if (lane == 0) masks[k * TILE + v] = vis;
         }
