@@ -39,9 +39,9 @@ MAX_BOUNCE = 3
 TAU_PAIRS = 65536
 # DRAM bytes (read + write) of one full gather launch of this workload, from the one-pass
 # capture `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum -k regex:gather_persistent
-# -s 3 -c 1 python bench.py --steps 1 --warmup 3 --skip-cpu` (37.58 MB read, 55.68 MB
+# -s 3 -c 1 python bench.py --steps 1 --warmup 3 --skip-cpu` (35.70 MB read, 57.40 MB
 # written; the writes are the per-chunk partial sums), recorded in profiles/.
-TRAFFIC_BYTES_PER_LAUNCH = (37.582336 + 55.679488) * 1e6
+TRAFFIC_BYTES_PER_LAUNCH = (35.6992 + 57.395968) * 1e6
 
 
 def workload_config():
