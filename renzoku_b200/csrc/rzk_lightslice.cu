@@ -1080,7 +1080,7 @@ rzk_status build(rzk_lightslice *L, const rzk_receiver *d_recv, const rzk_vpl *d
     return RZK_OK;
 }
 
-int cluster_gather_grid() {
+int cluster_vis_grid() {
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -1428,7 +1428,7 @@ rzk_status rzk_lightslice_gather(rzk_lightslice *L, const rzk_receiver *d_recv, 
         v.n_items = voff[ns];
         LS_TRY(cudaMemsetAsync(L->d_work.p, 0, sizeof(int), st));
         static int grid = 0;   // resident grid of the persistent kernel (one device per process)
-        if (grid == 0) grid = cluster_gather_grid();
+        if (grid == 0) grid = cluster_vis_grid();
         const DevScene ds = L->scene->dev();
         if (v.n_items > 0)
             cluster_vis_kernel<4, 32, 5><<<grid, 128, 0, st>>>(ds, L->d_perm.p, t, v, L->d_work.p);
