@@ -364,9 +364,15 @@ def run_ours(args):
         o = Oracle(sc)
         recv_np = rzk.records_from_device(recv_t, sg.RECEIVER_DTYPE)
         rng = np.random.default_rng(VPL_SEED)
-        samp = recv_np[np.sort(rng.choice(n_recv, 512, replace=False))].copy()
-        _, cnt = o.gather(samp, vpls_np, rzk.CLAMP_RADIANCE, tau, scale, cull=True,
-                          threads=os.cpu_count() or 1)
+        pick = np.sort(rng.choice(n_recv, 512, replace=False))
+        samp = recv_np[pick].copy()
+        ref32, ref64, cnt = o.gather(samp, vpls_np, rzk.CLAMP_RADIANCE, tau, scale, cull=True, f64=True,
+                                     threads=os.cpu_count() or 1)
+        # the timed image against the oracle (float and double) on the same sampled pixels
+        got = out.cpu().numpy()[pick]
+        parity = {"rel_l2_vs_oracle_f32": float(np.linalg.norm(got - ref32) / np.linalg.norm(ref32)),
+                  "rel_l2_vs_oracle_f64": float(np.linalg.norm(got - ref64) / np.linalg.norm(ref64)),
+                  "bound": 1e-3, "sample": "512 seeded shading points x all VPLs of the timed step"}
         pairs = samp.shape[0] * N_VPL
         trav = (32 * cnt["root_tests"] + 64 * cnt["inner_pops"] + 48 * cnt["leaf_tests"]) / pairs
         operand = 96.0 / 128 + 12.0 / N_VPL     # VPL record per 128-thread CTA, output per pair
@@ -415,6 +421,7 @@ def run_ours(args):
             "cpu_baseline": {"value": cpu_v, "unit": "evals/s", "cores": threads, "kind": kind,
                              "sample": f"{sample.shape[0]} seeded uniformly sampled shading points x {N_VPL} VPLs"},
             "clocks": clocks,
+            "parity": parity,
             "gpu_launches": launches_step * len(times),
             "gpu_launches_note": f"{launches_step} kernels per step, counted as the kernel nodes of one captured step",
             "tau": tau, "num_emitted": num_emitted, "bvh_build_s": build_s,
