@@ -142,6 +142,54 @@ rzk_status rzk_obj_get_info(const rzk_obj *obj, rzk_obj_info *info);
 rzk_status rzk_obj_scene_desc(const rzk_obj *obj, rzk_scene_desc *desc);
 rzk_status rzk_obj_destroy(rzk_obj *obj);
 
+/* JSON scenes -------------------------------------------------------------------------- */
+
+/* A scene file in the reference's JSON format, imported on the host: JsonImporter::load and
+ * get_scene (json_importer.cc:36-899) over JsonParser (json_parser.cc).  Sections are read in
+ * file order as the reference does ("geometry": OBJ meshes under <file's directory>/mesh/,
+ * "materials", "light_specs", "cameras", "scene": world surfaces binding meshes to
+ * materials, world lights binding meshes to area lights, views, options), giving the same
+ * surfaces in the same order with the same BSDF parameters and light radiances.  What this
+ * path does not model is counted and left out; the scene equals the reference's where those
+ * counts are 0. */
+typedef struct rzk_json rzk_json;
+enum { RZK_JSON_NONE = 0, RZK_JSON_PATH = 1, RZK_JSON_VPL = 2 };
+typedef struct {
+    int32_t n_prims, n_mats, n_lights;   /* the scene description's primitives, materials,
+                                            area lights */
+    int32_t has_camera;                  /* the first view whose integrator and camera resolve */
+    float eye[3], lookat[3], up[3];
+    float focal;                         /* "focal", else from "fov" over the film height
+                                            (Camera::focal_length_from_fov, camera.h:228-230) */
+    int32_t width, height;               /* "image" */
+    float film_w, film_h;                /* "film" */
+    float near_plane, far_plane;
+    int32_t integrator;                  /* that view's integrator: RZK_JSON_PATH or _VPL */
+    int32_t max_bounce, samples;
+    float tmin;                          /* options.geometry.tmin, else RAY_TMIN (1e-3) */
+    int32_t two_sided;                   /* options.geometry.two_sided_surfaces: every
+                                            primitive carries RZK_SURF_TWO_SIDED */
+    int32_t obj_files;                   /* OBJ files read */
+    int32_t point_lights, spot_lights, directional_lights;   /* not imported */
+    int32_t spheres;                     /* sphere surfaces and sphere area lights: not imported */
+    int32_t surfaces_unsupported_material;   /* glass, mirror, or a refractive or textured
+                                                OBJ material: left out */
+    int32_t skipped;                     /* entries the reference reports and skips (unknown
+                                            types, names that resolve to nothing) */
+    int32_t faces_with_vertex_normals;   /* summed over the OBJ files (rzk_obj_info) */
+    int32_t smoothed_faces;
+} rzk_json_info;
+
+/* Reads `path` and the OBJ and MTL files it names.  RZK_ERR_INVALID where the reference stops
+ * with an error: a file that cannot be read, a syntax error, a missing key or a value of the
+ * wrong type where the reference requires one. */
+rzk_status rzk_json_import(const char *path, rzk_json **out);
+rzk_status rzk_json_get_info(const rzk_json *js, rzk_json_info *info);
+/* Fills `desc` with pointers into the object (valid until rzk_json_destroy), ready for
+ * rzk_scene_create; tmin is the scene's. */
+rzk_status rzk_json_scene_desc(const rzk_json *js, rzk_scene_desc *desc);
+rzk_status rzk_json_destroy(rzk_json *js);
+
 /* Warm restart: a built scene as one host blob (device arrays and host-side counts), and
  * back.  No reference counterpart (the reference rebuilds its BVH from the scene file on
  * every run, aggregate_bvh.cc:48-240).  A restored scene answers every query bit for bit

@@ -281,6 +281,8 @@ class RefHarness:
             L.rref_matrix_save.argtypes = [P, I32, I32, ctypes.c_char_p]
             L.rref_obj_import.restype = I32
             L.rref_obj_import.argtypes = [ctypes.c_char_p, I32, P, P, P, P, P, P, P, P, P, P, P]
+            L.rref_json_import.restype = I32
+            L.rref_json_import.argtypes = [ctypes.c_char_p, I32, P, P, P, P, P, P, P, P, P, P, P, P, P, I32]
             L.rref_mrcs.restype = I32
             L.rref_mrcs.argtypes = [P, P, I32, I32, F32, U32, I32, F32, I32, P, I32, P, P, P, P, I32]
             cls._lib = L
@@ -394,6 +396,32 @@ class RefHarness:
         out = {"kind": kind[:k], "v": v[:k], "light": light[:k], "emit": emit[:k], "type": mtype[:k],
                "kd": kd[:k], "ks": ks[:k], "glossy": gl[:k]}
         return out, (cam if has_cam.value else None), n_surf.value
+
+    @classmethod
+    def json_import(cls, path, cap=100000, light_cap=100000):
+        """The reference's JsonImporter::load and get_scene on `path`: the per-surface fields
+        of obj_import plus each surface's two-sided flag, the first view's camera record (or
+        None), a dict of scene facts (surface count, integrator 1 path / 2 vpl, max_bounce,
+        samples, light counts by kind, two-sided option, tmin, near and far planes) and the
+        area lights' radiances in light-list order."""
+        kind = np.zeros(cap, np.int32); v = np.zeros((cap, 12), np.float32)
+        light = np.zeros(cap, np.int32); emit = np.zeros((cap, 3), np.float32)
+        mtype = np.zeros(cap, np.int32); kd = np.zeros((cap, 3), np.float32)
+        ks = np.zeros((cap, 3), np.float32); gl = np.zeros((cap, 2), np.float32)
+        two = np.zeros(cap, np.int32)
+        cam = np.zeros(1, sg.CAMERA_DTYPE)
+        meta = np.zeros(16, np.int32); fmeta = np.zeros(4, np.float32)
+        lemit = np.zeros((light_cap, 3), np.float32)
+        k = cls.lib().rref_json_import(str(path).encode(), cap, _ptr(kind), _ptr(v), _ptr(light), _ptr(emit),
+                                       _ptr(mtype), _ptr(kd), _ptr(ks), _ptr(gl), _ptr(two), _ptr(cam),
+                                       _ptr(meta), _ptr(fmeta), _ptr(lemit), light_cap)
+        out = {"kind": kind[:k], "v": v[:k], "light": light[:k], "emit": emit[:k], "type": mtype[:k],
+               "kd": kd[:k], "ks": ks[:k], "glossy": gl[:k], "two_sided": two[:k]}
+        facts = {"n_surfaces": int(meta[0]), "integrator": int(meta[2]), "max_bounce": int(meta[3]),
+                 "samples": int(meta[4]), "point_lights": int(meta[5]), "spot_lights": int(meta[6]),
+                 "directional_lights": int(meta[7]), "area_lights": int(meta[8]), "two_sided": int(meta[9]),
+                 "tmin": float(fmeta[0]), "near_plane": float(fmeta[1]), "far_plane": float(fmeta[2])}
+        return out, (cam if meta[1] else None), facts, lemit[:min(int(meta[8]), light_cap)]
 
     @classmethod
     def matrix_save(cls, mat, path):

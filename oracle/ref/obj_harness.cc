@@ -22,22 +22,10 @@ public:
 
 }  // namespace
 
-extern "C" {
+namespace rref {
 
-/* Imports `path` and writes, per surface whose shape is a triangle or quad (in surface
- * order, at most `cap`): kind (3 or 4), 12 vertex floats (p3 = 0 for a triangle), whether
- * it is a light, the light's radiance, and for a material its Bsdf::Type (0 Lambertian,
- * 1 Ward, 2 Phong; -1 any other BSDF), kd, ks and (n, 0) or (ax, ay).  cam (may be NULL) receives
- * the camera as rzk_camera when the scene has one.  Returns the number of such surfaces,
- * and the total surface count in *n_surfaces. */
-int rref_obj_import(const char *path, int cap, int32_t *kind, float *v, int32_t *is_light, float *emit,
-                    int32_t *mtype, float *kd, float *ks, float *gl, rzk_camera *cam, int32_t *has_cam,
-                    int32_t *n_surfaces) {
-    ObjImporter imp;
-    imp.load(path);
-    Surfaces surfaces;
-    imp.get_surfaces(surfaces);
-    *n_surfaces = (int32_t)surfaces.size();
+int flatten_surfaces(Surfaces &surfaces, int cap, int32_t *kind, float *v, int32_t *is_light, float *emit,
+                     int32_t *mtype, float *kd, float *ks, float *gl) {
     int k = 0;
     for (int i = 0; i < surfaces.size() && k < cap; ++i) {
         Surface &sf = surfaces[i];
@@ -75,24 +63,51 @@ int rref_obj_import(const char *path, int cap, int32_t *kind, float *v, int32_t 
         }
         k++;
     }
+    return k;
+}
+
+Rgb area_light_radiance(const AreaLight *l) { return LightProbe::radiance_of(l); }
+
+void camera_record(Camera *c, rzk_camera *cam) {
+    Sensor *sn = c->get_sensor();
+    Onb onb = c->get_onb();
+    put3(cam->eye, c->get_eye());
+    put3(cam->u, onb.u());
+    put3(cam->v, onb.v());
+    put3(cam->n, onb.n());
+    cam->focal = c->get_focal_length();
+    Vec2 cop = sn->get_cop();
+    Vec2 sc = sn->get_image_film_ratio();
+    cam->cop[0] = cop.x(); cam->cop[1] = cop.y();
+    cam->scale[0] = sc.x(); cam->scale[1] = sc.y();
+    cam->width = (int)sn->get_image_size().width;
+    cam->height = (int)sn->get_image_size().height;
+    cam->pad = 0;
+}
+
+}  // namespace rref
+
+extern "C" {
+
+/* Imports `path` and writes, per surface whose shape is a triangle or quad (in surface
+ * order, at most `cap`): kind (3 or 4), 12 vertex floats (p3 = 0 for a triangle), whether
+ * it is a light, the light's radiance, and for a material its Bsdf::Type (0 Lambertian,
+ * 1 Ward, 2 Phong; -1 any other BSDF), kd, ks and (n, 0) or (ax, ay).  cam (may be NULL) receives
+ * the camera as rzk_camera when the scene has one.  Returns the number of such surfaces,
+ * and the total surface count in *n_surfaces. */
+int rref_obj_import(const char *path, int cap, int32_t *kind, float *v, int32_t *is_light, float *emit,
+                    int32_t *mtype, float *kd, float *ks, float *gl, rzk_camera *cam, int32_t *has_cam,
+                    int32_t *n_surfaces) {
+    ObjImporter imp;
+    imp.load(path);
+    Surfaces surfaces;
+    imp.get_surfaces(surfaces);
+    *n_surfaces = (int32_t)surfaces.size();
+    const int k = flatten_surfaces(surfaces, cap, kind, v, is_light, emit, mtype, kd, ks, gl);
     *has_cam = 0;
     Scene *scene = imp.get_scene();   // NULL without a light or a camera
     if (scene && cam) {
-        Camera *c = scene->get_camera();
-        Sensor *sn = c->get_sensor();
-        Onb onb = c->get_onb();
-        put3(cam->eye, c->get_eye());
-        put3(cam->u, onb.u());
-        put3(cam->v, onb.v());
-        put3(cam->n, onb.n());
-        cam->focal = c->get_focal_length();
-        Vec2 cop = sn->get_cop();
-        Vec2 sc = sn->get_image_film_ratio();
-        cam->cop[0] = cop.x(); cam->cop[1] = cop.y();
-        cam->scale[0] = sc.x(); cam->scale[1] = sc.y();
-        cam->width = (int)sn->get_image_size().width;
-        cam->height = (int)sn->get_image_size().height;
-        cam->pad = 0;
+        camera_record(scene->get_camera(), cam);
         *has_cam = 1;
     }
     return k;

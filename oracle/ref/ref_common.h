@@ -100,6 +100,14 @@ struct HarnessEval : public IVirtualPointLightEvaluator {
     }
 };
 void fill_receiver(const Ray &r, const HitRecord &rec, rzk_receiver &out, const RefScene *s);
+/* obj_harness.cc: per surface whose shape is a triangle or quad, in order (at most cap):
+ * kind, 12 vertex floats, light flag, radiance, Bsdf::Type or -1, kd, ks, glossy pair;
+ * returns how many were written */
+int flatten_surfaces(Surfaces &surfaces, int cap, int32_t *kind, float *v, int32_t *is_light, float *emit,
+                     int32_t *mtype, float *kd, float *ks, float *gl);
+Rgb area_light_radiance(const AreaLight *l);
+/* obj_harness.cc: a Camera as rzk_camera */
+void camera_record(Camera *c, rzk_camera *cam);
 
 }  // namespace rref
 

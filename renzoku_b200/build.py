@@ -17,7 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "librzk_cuda.so")
 SOURCES = ["rzk_bvh.cu", "rzk_trace.cu", "rzk_gather.cu", "rzk_vplgen.cu", "rzk_capi.cu",
            "rzk_noalloc.cu", "rzk_cluster.cu", "rzk_batch.cu", "rzk_lightslice.cu", "rzk_guided.cu", "rzk_server.cu", "rzk_sah.cu", "rzk_mrcs.cu",
-           "rzk_serial.cu", "rzk_obj.cu"]
+           "rzk_serial.cu", "rzk_obj.cu", "rzk_json.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-fmad=false",
          "-prec-div=true", "-prec-sqrt=true", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off",

@@ -21,6 +21,7 @@
 // smoothing groups, which change the reference's shading normals, are counted and the
 // faces imported with their facet normals.
 #include "rzk_internal.cuh"
+#include "rzk_scenefile.h"
 
 #include <cstdio>
 #include <cstdlib>
@@ -29,9 +30,7 @@
 #include <vector>
 
 struct rzk_obj {
-    std::vector<int32_t> kind, mat, flags;
-    std::vector<float> v, emit;
-    std::vector<rzk_material> mats;
+    rzk::SceneArrays arrays;
     rzk_obj_info info;
 };
 
@@ -50,7 +49,7 @@ struct Mtl {
 
 struct Face {
     int v[4], n[4];
-    int count, mat, smooth;
+    int count, mat, smooth, object;
 };
 
 struct LightQuad {
@@ -167,19 +166,30 @@ bool to_material(const Mtl &m, rzk_material &out) {
     return true;
 }
 
-rzk_status import_obj(const char *path, rzk_obj *o) {
+void put_geometry(int count, const int *vi, const std::vector<float> &verts, int &kind, float *v) {
+    kind = count == 4 ? RZK_PRIM_QUAD : RZK_PRIM_TRIANGLE;
+    for (int k = 0; k < 4; ++k)
+        for (int c = 0; c < 3; ++c) v[3 * k + c] = k < count ? verts[3 * vi[k] + c] : 0.0f;
+}
+
+}  // namespace
+
+namespace rzk {
+
+rzk_status obj_load(const char *path, ObjModel &o) {
     FILE *f = std::fopen(path, "r");
     if (!f) return RZK_ERR_INVALID;
     std::vector<float> verts, normals;   // 3 per vertex / normal
-    int n_tex = 0;
     std::vector<Face> faces;
     std::vector<LightQuad> lquads;
+    std::vector<int> sphere_mats;
     std::vector<Mtl> mtls;
-    int cur_mat = -1, cur_smooth = 0;
+    int cur_mat = -1, cur_smooth = 0, cur_object = -1;
     bool have_cam = false, bad = false;
     int cam_idx[3] = {0, 0, 0};
     float focal = 0.0f;
-    rzk_obj_info &info = o->info;
+    std::memset(&o.info, 0, sizeof(o.info));
+    rzk_obj_info &info = o.info;
     std::string dir(path);
     const size_t slash = dir.find_last_of("/\\");
     dir = slash == std::string::npos ? std::string() : dir.substr(0, slash + 1);
@@ -190,8 +200,6 @@ rzk_status import_obj(const char *path, rzk_obj *o) {
         if (!std::strcmp(tok, "v") || !std::strcmp(tok, "vn")) {
             std::vector<float> &dst = tok[1] ? normals : verts;
             for (int c = 0; c < 3; ++c) dst.push_back(next_real(kSpace));
-        } else if (!std::strcmp(tok, "vt")) {
-            n_tex++;
         } else if (!std::strcmp(tok, "f")) {
             Face fc;
             std::memset(&fc, 0, sizeof(fc));
@@ -202,6 +210,7 @@ rzk_status import_obj(const char *path, rzk_obj *o) {
             }
             fc.mat = cur_mat;
             fc.smooth = cur_smooth;
+            fc.object = cur_object;
             faces.push_back(fc);
         } else if (!std::strcmp(tok, "lq")) {
             LightQuad q;
@@ -213,6 +222,11 @@ rzk_status import_obj(const char *path, rzk_obj *o) {
             info.point_lights++;
         } else if (!std::strcmp(tok, "sp")) {
             info.spheres++;
+            sphere_mats.push_back(cur_mat);
+        } else if (!std::strcmp(tok, "o")) {   // object name (obj_parser.cpp:527-532)
+            const char *name = std::strtok(nullptr, kSpace);
+            o.object_names.push_back(name ? name : "");
+            cur_object++;
         } else if (!std::strcmp(tok, "c")) {
             int k = 0;
             const char *t;
@@ -251,7 +265,7 @@ rzk_status import_obj(const char *path, rzk_obj *o) {
             const char *g = std::strtok(nullptr, kSpace);
             cur_smooth = (!g || !std::strcmp(g, "off")) ? 0 : (int)std::atof(g);
         }
-        // o, g, p, pl, ld and unknown commands: nothing this path reads
+        // vt, g, p, pl, ld and unknown commands: nothing this path reads
     }
     std::fclose(f);
     if (bad) return RZK_ERR_INVALID;
@@ -265,22 +279,13 @@ rzk_status import_obj(const char *path, rzk_obj *o) {
     for (size_t i = 0; i < mtls.size(); ++i) {
         rzk_material m;
         if (to_material(mtls[i], m)) {
-            mat_of[i] = (int)o->mats.size();
-            o->mats.push_back(m);
+            mat_of[i] = (int)o.mats.size();
+            o.mats.push_back(m);
         }
+        o.mtl_names.push_back(mtls[i].name);
     }
+    o.mtl_mats = mat_of;
     const int nv = (int)(verts.size() / 3);
-    auto push = [&](int count, const int *vi, int mat, const float *emit) {
-        o->kind.push_back(count == 4 ? RZK_PRIM_QUAD : RZK_PRIM_TRIANGLE);
-        for (int k = 0; k < 4; ++k) {
-            const int idx = vi[k < count ? k : 0];
-            for (int c = 0; c < 3; ++c) o->v.push_back(k < count ? verts[3 * idx + c] : 0.0f);
-        }
-        o->mat.push_back(mat);
-        o->flags.push_back(0);
-        for (int c = 0; c < 3; ++c) o->emit.push_back(emit ? emit[c] : 0.0f);
-        if (mat < 0) info.n_lights++;
-    };
     auto in_range = [&](int count, const int *vi) {
         for (int k = 0; k < count; ++k)
             if (vi[k] < 0 || vi[k] >= nv) return false;
@@ -289,47 +294,116 @@ rzk_status import_obj(const char *path, rzk_obj *o) {
     // light quads (obj_importer.cc:271-284): radiance = the material's diffuse colour
     for (const LightQuad &q : lquads) {
         if (q.count != 4 || q.mat < 0 || !in_range(4, q.v)) return RZK_ERR_INVALID;
-        push(4, q.v, -1, mtls[q.mat].diff);
+        ObjSurface sf;
+        std::memset(&sf, 0, sizeof(sf));
+        sf.type = OBJ_SURF_LIGHT;
+        sf.shape = -1;
+        sf.mat = -1;
+        put_geometry(4, q.v, verts, sf.kind, sf.v);
+        for (int c = 0; c < 3; ++c) sf.emit[c] = mtls[q.mat].diff[c];
+        o.surfaces.push_back(sf);
     }
-    // faces (obj_importer.cc:306-452)
+    // faces (obj_importer.cc:306-452): each face of 3 or 4 vertices is a shape; one with a
+    // material is also a surface
     for (const Face &fc : faces) {
         if (fc.count < 3) { info.short_faces++; continue; }
         if (!in_range(fc.count, fc.v)) return RZK_ERR_INVALID;
-        bool normals_given = false;
-        for (int k = 0; k < fc.count; ++k) normals_given |= fc.n[k] >= 0;
-        if (fc.mat < 0) { info.faces_without_material++; continue; }
+        ObjShape sh;
+        put_geometry(fc.count, fc.v, verts, sh.kind, sh.v);
+        sh.object = fc.object;
+        sh.surface = -1;
+        if (fc.mat < 0) {
+            info.faces_without_material++;
+            o.shapes.push_back(sh);
+            continue;
+        }
         const Mtl &m = mtls[fc.mat];
+        ObjSurface sf;
+        std::memset(&sf, 0, sizeof(sf));
+        sf.kind = sh.kind;
+        std::memcpy(sf.v, sh.v, sizeof(sf.v));
+        sf.mat = -1;
         if (is_light_name(m.name)) {
-            if (m.refract_index > 1.0f) { info.faces_unsupported_material++; continue; }
-            push(fc.count, fc.v, -1, m.diff);
+            // a light needs a diffuse BSDF (obj_importer.cc:427-435): not a refractive one
+            if (m.refract_index > 1.0f) {
+                info.faces_unsupported_material++;
+                o.shapes.push_back(sh);
+                continue;
+            }
+            sf.type = OBJ_SURF_LIGHT;
+            for (int c = 0; c < 3; ++c) sf.emit[c] = m.diff[c];
         } else if (mat_of[fc.mat] < 0) {
             info.faces_unsupported_material++;
-            continue;
+            sf.type = OBJ_SURF_UNSUPPORTED;
         } else {
-            push(fc.count, fc.v, mat_of[fc.mat], nullptr);
+            sf.type = OBJ_SURF_MATERIAL;
+            sf.mat = mat_of[fc.mat];
         }
-        if (normals_given) info.faces_with_vertex_normals++;
-        else if (fc.smooth > 0) info.smoothed_faces++;
+        if (sf.type != OBJ_SURF_UNSUPPORTED) {
+            bool normals_given = false;
+            for (int k = 0; k < fc.count; ++k) normals_given |= fc.n[k] >= 0;
+            if (normals_given) info.faces_with_vertex_normals++;
+            else if (fc.smooth > 0) info.smoothed_faces++;
+        }
+        sh.surface = (int)o.surfaces.size();
+        sf.shape = (int)o.shapes.size();
+        o.shapes.push_back(sh);
+        o.surfaces.push_back(sf);
     }
-    info.n_prims = (int)o->kind.size();
-    info.n_mats = (int)o->mats.size();
-    (void)n_tex;
+    // spheres (obj_importer.cc:455-468): surfaces after the faces
+    for (size_t i = 0; i < sphere_mats.size(); ++i) {
+        ObjSurface sf;
+        std::memset(&sf, 0, sizeof(sf));
+        sf.type = OBJ_SURF_SPHERE;
+        sf.shape = -1;
+        sf.mat = -1;
+        o.surfaces.push_back(sf);
+    }
+    for (const ObjSurface &sf : o.surfaces) {
+        if (sf.type == OBJ_SURF_MATERIAL || sf.type == OBJ_SURF_LIGHT) info.n_prims++;
+        if (sf.type == OBJ_SURF_LIGHT) info.n_lights++;
+    }
+    info.n_mats = (int)o.mats.size();
     return RZK_OK;
 }
 
-}  // namespace
+void SceneArrays::add(int k, const float *v12, int m, const float *e, int f) {
+    kind.push_back(k);
+    v.insert(v.end(), v12, v12 + 12);
+    mat.push_back(m);
+    flags.push_back(f);
+    for (int c = 0; c < 3; ++c) emit.push_back(e ? e[c] : 0.0f);
+}
+
+void SceneArrays::desc(rzk_scene_desc *d, float tmin) const {
+    std::memset(d, 0, sizeof(*d));
+    d->n_prims = (int32_t)kind.size();
+    d->prim_kind = kind.data();
+    d->prim_v = v.data();
+    d->prim_mat = mat.data();
+    d->prim_emit = emit.data();
+    d->prim_flags = flags.data();
+    d->n_mats = (int32_t)mats.size();
+    d->mats = mats.data();
+    d->tmin = tmin;
+}
+
+}  // namespace rzk
 
 extern "C" {
 
 rzk_status rzk_obj_import(const char *path, rzk_obj **out) {
     if (!path || !out) return RZK_ERR_INVALID;
     *out = nullptr;
+    rzk::ObjModel m;
+    const rzk_status r = rzk::obj_load(path, m);
+    if (r != RZK_OK) return r;
     rzk_obj *o = new rzk_obj();
-    std::memset(&o->info, 0, sizeof(o->info));
-    const rzk_status r = import_obj(path, o);
-    if (r != RZK_OK) {
-        delete o;
-        return r;
+    o->info = m.info;
+    o->arrays.mats = m.mats;
+    for (const rzk::ObjSurface &sf : m.surfaces) {
+        if (sf.type == rzk::OBJ_SURF_MATERIAL) o->arrays.add(sf.kind, sf.v, sf.mat, nullptr, 0);
+        else if (sf.type == rzk::OBJ_SURF_LIGHT) o->arrays.add(sf.kind, sf.v, -1, sf.emit, 0);
     }
     *out = o;
     return RZK_OK;
@@ -343,16 +417,7 @@ rzk_status rzk_obj_get_info(const rzk_obj *obj, rzk_obj_info *info) {
 
 rzk_status rzk_obj_scene_desc(const rzk_obj *obj, rzk_scene_desc *desc) {
     if (!obj || !desc) return RZK_ERR_INVALID;
-    std::memset(desc, 0, sizeof(*desc));
-    desc->n_prims = (int32_t)obj->kind.size();
-    desc->prim_kind = obj->kind.data();
-    desc->prim_v = obj->v.data();
-    desc->prim_mat = obj->mat.data();
-    desc->prim_emit = obj->emit.data();
-    desc->prim_flags = obj->flags.data();
-    desc->n_mats = (int32_t)obj->mats.size();
-    desc->mats = obj->mats.data();
-    desc->tmin = 1e-3f;
+    obj->arrays.desc(desc, 1e-3f);
     return RZK_OK;
 }
 

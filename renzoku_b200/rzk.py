@@ -64,6 +64,10 @@ SIGNATURES = [
     ("rzk_obj_get_info", I32, [P, P]),
     ("rzk_obj_scene_desc", I32, [P, P]),
     ("rzk_obj_destroy", I32, [P]),
+    ("rzk_json_import", I32, [ctypes.c_char_p, P]),
+    ("rzk_json_get_info", I32, [P, P]),
+    ("rzk_json_scene_desc", I32, [P, P]),
+    ("rzk_json_destroy", I32, [P]),
     ("rzk_vpl_generate", I32, [P, U32, I32, I32, P, I32, P, P]),
     ("rzk_gather", I32, [P, P, P, I32, P, I32, I32, F32, F32, P, P]),
     ("rzk_gather_variants", I32, []),
@@ -241,36 +245,67 @@ class ObjInfoC(ctypes.Structure):
                 ("faces_with_vertex_normals", I32), ("smoothed_faces", I32), ("mtl_files_missing", I32)]
 
 
+def _scene_from_desc(name: str, d, info):
+    """A scenegen.Scene copied out of a filled rzk_scene_desc, with the info's camera."""
+    n, m = d.n_prims, d.n_mats
+
+    def arr(ptr, dtype, count):
+        if count == 0:
+            return np.zeros(0, dtype)
+        return np.frombuffer(ctypes.string_at(ptr, np.dtype(dtype).itemsize * count), dtype).copy()
+
+    spec = sg.CameraSpec(tuple(info.eye), tuple(info.lookat), tuple(info.up), float("nan"), info.width,
+                         info.height, info.film_w, info.film_h)
+    return sg.Scene(name, arr(d.prim_kind, np.int32, n),
+                    arr(d.prim_v, np.float32, 12 * n).reshape(n, 12), arr(d.prim_mat, np.int32, n),
+                    arr(d.prim_emit, np.float32, 3 * n).reshape(n, 3), arr(d.prim_flags, np.int32, n),
+                    arr(d.mats, sg.MATERIAL_DTYPE, m), spec, d.tmin)
+
+
+def _import_scene_file(path, kind: str, info_cls):
+    lib = load()
+    h = ctypes.c_void_p()
+    check(getattr(lib, f"rzk_{kind}_import")(str(path).encode(), ctypes.byref(h)), f"rzk_{kind}_import")
+    try:
+        info = info_cls()
+        check(getattr(lib, f"rzk_{kind}_get_info")(h, ctypes.byref(info)), f"rzk_{kind}_get_info")
+        d = sg.SceneDescC()
+        check(getattr(lib, f"rzk_{kind}_scene_desc")(h, ctypes.byref(d)), f"rzk_{kind}_scene_desc")
+        scene = _scene_from_desc(os.path.splitext(os.path.basename(str(path)))[0], d, info)
+        cam = (Camera.from_focal(info.eye, info.lookat, info.up, info.focal, info.width, info.height,
+                                 info.film_w, info.film_h) if info.has_camera else None)
+        out = {k: getattr(info, k) for k, _ in info_cls._fields_ if k not in ("eye", "lookat", "up")}
+        return scene, cam, out
+    finally:
+        getattr(lib, f"rzk_{kind}_destroy")(h)
+
+
 def import_obj(path: str):
     """A Wavefront OBJ scene in the reference's dialect (rzk_obj_import): returns
     (scenegen.Scene, Camera or None, info dict of what was counted and left out)."""
-    lib = load()
-    h = ctypes.c_void_p()
-    check(lib.rzk_obj_import(str(path).encode(), ctypes.byref(h)), "rzk_obj_import")
-    try:
-        info = ObjInfoC()
-        check(lib.rzk_obj_get_info(h, ctypes.byref(info)), "rzk_obj_get_info")
-        d = sg.SceneDescC()
-        check(lib.rzk_obj_scene_desc(h, ctypes.byref(d)), "rzk_obj_scene_desc")
-        n, m = d.n_prims, d.n_mats
+    return _import_scene_file(path, "obj", ObjInfoC)
 
-        def arr(ptr, dtype, count):
-            if count == 0:
-                return np.zeros(0, dtype)
-            return np.frombuffer(ctypes.string_at(ptr, np.dtype(dtype).itemsize * count), dtype).copy()
 
-        spec = sg.CameraSpec(tuple(info.eye), tuple(info.lookat), tuple(info.up), float("nan"), info.width,
-                             info.height, info.film_w, info.film_h)
-        scene = sg.Scene(os.path.splitext(os.path.basename(str(path)))[0], arr(d.prim_kind, np.int32, n),
-                         arr(d.prim_v, np.float32, 12 * n).reshape(n, 12), arr(d.prim_mat, np.int32, n),
-                         arr(d.prim_emit, np.float32, 3 * n).reshape(n, 3), arr(d.prim_flags, np.int32, n),
-                         arr(d.mats, sg.MATERIAL_DTYPE, m), spec, d.tmin)
-        cam = (Camera.from_focal(info.eye, info.lookat, info.up, info.focal, info.width, info.height,
-                                 info.film_w, info.film_h) if info.has_camera else None)
-        out = {k: getattr(info, k) for k, _ in ObjInfoC._fields_ if k not in ("eye", "lookat", "up")}
-        return scene, cam, out
-    finally:
-        lib.rzk_obj_destroy(h)
+class JsonInfoC(ctypes.Structure):
+    """ctypes mirror of rzk_json_info."""
+    _fields_ = [("n_prims", I32), ("n_mats", I32), ("n_lights", I32), ("has_camera", I32),
+                ("eye", F32 * 3), ("lookat", F32 * 3), ("up", F32 * 3), ("focal", F32),
+                ("width", I32), ("height", I32), ("film_w", F32), ("film_h", F32),
+                ("near_plane", F32), ("far_plane", F32), ("integrator", I32), ("max_bounce", I32),
+                ("samples", I32), ("tmin", F32), ("two_sided", I32), ("obj_files", I32),
+                ("point_lights", I32), ("spot_lights", I32), ("directional_lights", I32), ("spheres", I32),
+                ("surfaces_unsupported_material", I32), ("skipped", I32), ("faces_with_vertex_normals", I32),
+                ("smoothed_faces", I32)]
+
+
+JSON_INTEGRATORS = {0: None, 1: "path", 2: "vpl"}
+
+
+def import_json(path: str):
+    """A scene file in the reference's JSON format (rzk_json_import; JsonImporter::load and
+    get_scene, json_importer.cc): returns (scenegen.Scene, Camera or None, info dict with the
+    first view's integrator, max_bounce and samples and what was counted and left out)."""
+    return _import_scene_file(path, "json", JsonInfoC)
 
 
 class AggregateCuda:

@@ -369,3 +369,75 @@ def write_obj(scene: Scene, path: str) -> None:
             name = f"rz_light_{light_of[p]}" if scene.prim_mat[p] < 0 else f"mat_{int(scene.prim_mat[p])}"
             f.write(f"usemtl {name}\n")
             f.write("f " + " ".join(str(-n + j) for j in range(n)) + "\n")
+
+
+def write_json(scene: Scene, path: str, integrator: str = "vpl", max_bounce: int = 3, samples: int = 1,
+               tmin=None, two_sided=None) -> None:
+    """Writes `scene` as a scene file in the reference's JSON format (json_importer.cc) with
+    its geometry in one OBJ file without materials (mesh/<name>.obj beside it, one `o` object
+    per material, `m<i>`, and per emitter, `e<k>`), which rzk_json_import reads back:
+    materials `mat_<i>` (lambertian kd; phong kd, ks, n; ward kd, ks, ax, ay), area light
+    specs `area_<k>` with each emitter's radiance, world surfaces binding `<name>.m<i>` to
+    `mat_<i>`, world lights binding `<name>.e<k>` to `area_<k>`, a pinhole camera from the
+    scene's camera (fov) and one view with the given integrator.  Reals are written with 9
+    significant digits, so float32 values read back unchanged; the surfaces come back grouped
+    by material, then the emitters."""
+    import json
+    import os
+    root = os.path.dirname(os.path.abspath(path))
+    name = os.path.splitext(os.path.basename(path))[0]
+    os.makedirs(os.path.join(root, "mesh"), exist_ok=True)
+    g = lambda x: "%.9g" % float(x)
+    lights = np.nonzero(scene.prim_mat < 0)[0]
+    with open(os.path.join(root, "mesh", name + ".obj"), "w") as f:
+        def put(p):
+            n = int(scene.prim_kind[p])
+            for j in range(n):
+                f.write("v " + " ".join(g(x) for x in scene.prim_v[p, 3 * j:3 * j + 3]) + "\n")
+            f.write("f " + " ".join(str(-n + j) for j in range(n)) + "\n")
+        for i in range(len(scene.mats)):
+            f.write(f"o m{i}\n")
+            for p in np.nonzero(scene.prim_mat == i)[0]:
+                put(p)
+        for k, p in enumerate(lights):
+            f.write(f"o e{k}\n")
+            put(p)
+    num = lambda x: json.loads(g(x))
+    mats = {}
+    for i, m in enumerate(scene.mats):
+        t = int(m["type"])
+        spec = {"kd": [num(x) for x in m["kd"]]}
+        if t == BSDF_PHONG:
+            spec.update(type="phong", ks=[num(x) for x in m["ks"]], n=num(m["p0"]))
+        elif t == BSDF_WARD:
+            spec.update(type="ward", ks=[num(x) for x in m["ks"]], ax=num(m["p0"]), ay=num(m["p1"]))
+        else:
+            spec["type"] = "lambertian"
+        mats[f"mat_{i}"] = {"type": spec.pop("type"), **spec}
+    cam = scene.camera
+    doc = {
+        "geometry": {name: name + ".obj"},
+        "materials": mats,
+        "light_specs": {f"area_{k}": {"type": "area", "radiance": [num(x) for x in scene.prim_emit[p]]}
+                        for k, p in enumerate(lights)},
+        "cameras": {"cam": {"type": "pinhole", "pos": [num(x) for x in cam.eye],
+                            "lookat": [num(x) for x in cam.lookat], "up": [num(x) for x in cam.up],
+                            "near": 0.01, "far": 100.0, "image": [int(cam.width), int(cam.height)],
+                            "film": [num(cam.film_w), num(cam.film_h)], "fov": num(cam.fov)}},
+        "scene": {
+            "world": {
+                "surfaces": {f"s{i}": {"mesh": f"{name}.m{i}", "bsdf": f"mat_{i}"} for i in range(len(scene.mats))},
+                "lights": {f"l{k}": {"light": f"area_{k}", "mesh": f"{name}.e{k}"} for k in range(len(lights))},
+            },
+            "views": {"main": {"camera": "cam", "integrator": {"type": integrator, "max_bounce": int(max_bounce),
+                                                               "samples": int(samples)}}},
+            "options": {"geometry": {"traversal": "bvh"}},
+        },
+    }
+    geo = doc["scene"]["options"]["geometry"]
+    if tmin is not None:
+        geo["tmin"] = num(tmin)
+    if two_sided is not None:
+        geo["two_sided_surfaces"] = bool(two_sided)
+    with open(path, "w") as f:
+        json.dump(doc, f, indent=1)

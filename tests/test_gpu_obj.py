@@ -1,6 +1,7 @@
-"""A scene read by rzk_obj_import goes through the device path like a generated one: a
-room written with scenegen.write_obj and read back renders its primary hits and its
-gather bit for bit like the oracle (all-Lambertian, one VPL chunk)."""
+"""A scene read by rzk_obj_import or rzk_json_import goes through the device path like a
+generated one: a room written with scenegen.write_obj or write_json and read back renders its
+primary hits (through the imported camera, for JSON) and its gather bit for bit like the
+oracle (all-Lambertian, one VPL chunk)."""
 import numpy as np
 import pytest
 
@@ -9,14 +10,20 @@ from renzoku_b200 import scenegen as sg
 pytestmark = pytest.mark.gpu
 
 
-def test_imported_obj_scene_renders_like_the_oracle(ctx, oracle_built, tmp_path):
+@pytest.mark.parametrize("fmt", ["obj", "json"])
+def test_imported_scene_renders_like_the_oracle(ctx, oracle_built, tmp_path, fmt):
     from oracle import Oracle
     from renzoku_b200 import rzk
     src = sg.room_boxes(64, 64)
-    sg.write_obj(src, str(tmp_path / "room.obj"))
-    scene, _, info = rzk.import_obj(str(tmp_path / "room.obj"))
+    if fmt == "obj":
+        sg.write_obj(src, str(tmp_path / "room.obj"))
+        scene, _, info = rzk.import_obj(str(tmp_path / "room.obj"))
+        cam = rzk.Camera(src.camera)
+    else:
+        sg.write_json(src, str(tmp_path / "room.json"))
+        scene, cam, info = rzk.import_json(str(tmp_path / "room.json"))
+        assert cam is not None and info["integrator"] == 2
     assert scene.n_prims == src.n_prims
-    cam = rzk.Camera(src.camera)
     agg = rzk.AggregateCuda(ctx, scene)
     o = Oracle(scene)
     recv_t = agg.primary(cam)
