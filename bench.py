@@ -766,7 +766,7 @@ def run_guided(args):
     spp = args.spp
 
     def step():
-        ls.guided_render(cam, spp, 8, rr_depth=3, rr_prob=0.5, seed=VPL_SEED, out=out)
+        ls.guided_render(cam, spp, 8, rr_depth=3, rr_prob=0.5, seed=VPL_SEED, out=out, sampler=args.sampler)
 
     for _ in range(args.warmup):
         step()
@@ -787,12 +787,15 @@ def run_guided(args):
     ms = 1e3 * sum(times) / len(times)
     paths = cam.n_pixels * spp
     line = {
-        "metric": "guided path-tracing paths/s (LightSlice Jensen-map guiding, MIS with BRDF sampling)",
+        "metric": ("guided path-tracing paths/s (LightSlice " +
+                   ("Jensen-map" if args.sampler == "jensen" else "Metropolis-chain") +
+                   " guiding, MIS with BRDF sampling)"),
         "value": paths / (ms / 1e3), "unit": "paths/s", "n_gpus": 1, "steps": len(times),
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"guided_pt_room_spheres_{agg.n_tris}_tris_{side}x{side}_{spp}spp_depth8_rr3",
-                   "triangles": agg.n_tris, "spp": spp, "max_bounce": 8, "rr_depth": 3, "rr_prob": 0.5,
+        "config": {"workload": f"guided_pt_room_spheres_{agg.n_tris}_tris_{side}x{side}_{spp}spp_depth8_rr3"
+                               + ("" if args.sampler == "jensen" else "_metropolis"),
+                   "sampler": args.sampler, "triangles": agg.n_tris, "spp": spp, "max_bounce": 8, "rr_depth": 3, "rr_prob": 0.5,
                    "vpls": n_vpl, "vpls_used": info["vpls_used"], "global_clusters": info["global_clusters"],
                    "slices": info["slices"], "slice_clusters": info["slice_clusters"], "map_resolution": 32,
                    "max_slice_size": args.slice_size,
@@ -940,6 +943,8 @@ def main():
                          "scene build vs restore from a blob (1 GPU); guided: "
                          "LightSlice-guided path tracing, 1024^2 x 16 spp (1 GPU)")
     ap.add_argument("--spp", type=int, default=16)
+    ap.add_argument("--sampler", choices=["jensen", "metropolis"], default="jensen",
+                    help="guided: LightSlice's direction sampler")
     ap.add_argument("--side", type=int, default=1024)
     ap.add_argument("--max-slice-clusters", type=int, default=4096)
     ap.add_argument("--slice-size", type=int, default=4096)

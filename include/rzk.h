@@ -516,17 +516,40 @@ typedef struct {
     float rr_prob;            /* survival probability when Russian roulette applies */
     int32_t direct_lighting;  /* Integrator::is_direct_lighting */
     uint32_t seed;            /* sample s of pixel k draws from stream (seed, 6, k * spp + s) */
+    int32_t sampler;          /* LightSlice's direction sampler: RZK_GUIDE_JENSEN (0) or
+                                 RZK_GUIDE_METROPOLIS (1, the reference's default) */
+    int32_t chain_samples;    /* METROPOLIS: chain states kept per slice after the warm-up
+                                 (0: 4096) */
 } rzk_guided_params;
+enum { RZK_GUIDE_JENSEN = 0, RZK_GUIDE_METROPOLIS = 1 };
 
 /* VirtualPointLight::guided_path_trace / trace_wellington with METRO_RANDOM
- * (vpl.cc:907-1040) guided by a LightSlice's Jensen maps (LightSlice::sample / pdf with
- * sampling_type JENSEN, lightslice.cc:1569-2056, 2313-2377) and FirstBounce::radiance for
+ * (vpl.cc:907-1040) guided by a LightSlice (LightSlice::sample / pdf, lightslice.cc:1569-2056)
+ * with its JENSEN sampler (the slice's luminance map, lightslice.cc:2313-2377) or its
+ * METROPOLIS sampler (Metropolis chains over each slice's incoming-radiance density,
+ * lightslice.cc:1427-1517, 1709-1928: eight per slice, each with the reference's 1,024-state
+ * warm-up, run before the paths from the streams (seed, 8, slice * 8 + chain), and a path
+ * draws a state of its slice's chains uniformly, so the directions match the reference's in
+ * distribution only) and FirstBounce::radiance for
  * direct light (first_bounce.h:54-71, area_light.cc:48-142).  Russian roulette (rr_depth,
  * rr_prob) has no reference counterpart: the reference recursion always runs to
  * max_bounce.  Writes the per-pixel mean over spp (d_rgb [W*H][3]) and optionally every
  * path's radiance (d_paths [W*H*spp][3], path = pixel * spp + sample). */
 rzk_status rzk_guided_render(rzk_context *ctx, rzk_scene *scene, rzk_lightslice *ls, const rzk_camera *camera,
                              const rzk_guided_params *params, float *d_rgb, float *d_paths, void *stream);
+/* LightSlice::eval_incoming_radiance (FIXED_RADIUS, lightslice.cc:1427-1517): the METROPOLIS
+ * sampler's density of slice d_slice[i] at the point (d_xy[2i], d_xy[2i+1]) of the unit
+ * square of that slice's sampling record, into d_out[i] (0 for a slice out of range). */
+rzk_status rzk_lightslice_density(rzk_lightslice *ls, const int32_t *d_slice, const float *d_xy, int n, float *d_out,
+                                  void *stream);
+/* The METROPOLIS chains rzk_guided_render draws from (LightSlice::metropolis_sample,
+ * lightslice.cc:1763-1911): per slice eight chains from the streams (seed, 8, slice * 8 +
+ * chain), each 1,024 warm-up states (the first a cluster drawn from the slice's cluster
+ * distribution) and then its eighth of the slice's n_samples states in order, each as
+ * (x, y, density, 0) with (x, y) its point on the unit square of the slice's sampling record
+ * (direction_to_square), into d_out [n_slices][n_samples][4]; zeros for a slice without a
+ * valid sampling record. */
+rzk_status rzk_lightslice_chains(rzk_lightslice *ls, uint32_t seed, int n_samples, float *d_out, void *stream);
 
 /* Serving ---------------------------------------------------------------------------- */
 

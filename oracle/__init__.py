@@ -278,6 +278,8 @@ class RefHarness:
             L.rref_ls_maps.argtypes = [P, P, P, P, P]
             L.rref_ls_gather.argtypes = [P, P, I32, I32, F32, P]
             L.rref_ls_guided.argtypes = [P, P, I32, I32, I32, I32, F32, I32, U32, P]
+            L.rref_ls_density.argtypes = [P, P, P, I32, P]
+            L.rref_ls_set_sampler.argtypes = [P, I32]
             L.rref_matrix_save.argtypes = [P, I32, I32, ctypes.c_char_p]
             L.rref_obj_import.restype = I32
             L.rref_obj_import.argtypes = [ctypes.c_char_p, I32, P, P, P, P, P, P, P, P, P, P, P]
@@ -552,8 +554,18 @@ class RefLightSlice:
         return out
 
 
-    def guided(self, pixels, spp, max_bounce, rr_depth=0, rr_prob=1.0, direct=True, seed=2013):
-        """Per-path radiance [len(pixels)][spp][3] of the reference's guided path tracer."""
+    def density(self, slices, xy):
+        """LightSlice::eval_incoming_radiance (the METROPOLIS density) of slices[i] at xy[i]."""
+        sl = np.ascontiguousarray(slices, np.int32)
+        pts = np.ascontiguousarray(xy, np.float32).reshape(-1, 2)
+        out = np.zeros(len(sl), np.float32)
+        RefHarness.lib().rref_ls_density(self.h, _ptr(sl), _ptr(pts), len(sl), _ptr(out))
+        return out
+
+    def guided(self, pixels, spp, max_bounce, rr_depth=0, rr_prob=1.0, direct=True, seed=2013, sampler="jensen"):
+        """Per-path radiance [len(pixels)][spp][3] of the reference's guided path tracer with
+        its "jensen" or "metropolis" sampler (the Metropolis chains start afresh each call)."""
+        RefHarness.lib().rref_ls_set_sampler(self.h, {"jensen": 0, "metropolis": 1}[sampler])
         pixels = np.ascontiguousarray(pixels, np.int32)
         out = np.zeros((len(pixels), spp, 3), np.float32)
         RefHarness.lib().rref_ls_guided(self.h, _ptr(pixels), len(pixels), spp, max_bounce, rr_depth, rr_prob,

@@ -88,6 +88,8 @@ struct RefLs {
     BrdfPointLights vpls1;
     HarnessEval ev;
     int k = 16;
+    int sampler = 0;          // 0 JENSEN, 1 METROPOLIS
+    bool metro_ready = false;
 };
 
 Receiver rep_receiver(RefLs *h, int s) {
@@ -490,6 +492,68 @@ static Rgb ref_trace(RefLs *h, const Receiver &r, int bounce, int max_bounce, in
     return radiance;
 }
 
+/* The METROPOLIS sampler's set-up, as LightSlice::initialize runs it after the maps
+ * (lightslice.cc:1180-1262, restated here around the reference's types): a KdTree2 per slice
+ * over its visible clusters' directions on the unit square of its sampling record, and each
+ * record's chain reset with sum_f = sum_vpl (FIXED_RADIUS).  Runs once. */
+static void metro_prepare(RefLs *h) {
+    if (h->metro_ready) return;
+    LightSlice *ls = h->ls;
+    for (int s = 0; s < (int)ls->matrix_clusters.size(); ++s) {
+        const int slice = s;
+        int n = 0;
+        for (size_t c = 0; c < ls->matrix_clusters[slice].size(); ++c)
+            if (ls->matrix_clusters[slice][c].is_upper_hemisphere) n++;
+        ls->slices[s].tree_node_data = new NodeData2[n];
+        NodeData2 *data = ls->slices[s].tree_node_data;
+        n = 0;
+        if (!ls->sampling_records[slice].is_valid) continue;
+        for (size_t c = 0; c < ls->matrix_clusters[slice].size(); ++c) {
+            if (!ls->matrix_clusters[slice][c].is_upper_hemisphere) continue;
+            Vec3 local_wi = ls->sampling_records[s].uvn.world_to_local(ls->matrix_clusters[slice][c].slice_wi);
+            if (local_wi.z() <= 0.0f) continue;
+            data[n].p = direction_to_square(local_wi);
+            data[n].index = slice * ls->max_slice_clusters + (int)c;
+            n++;
+        }
+        ls->slices[s].kdtree = new KdTree2(data, n, ls->scene);
+    }
+    for (int s = 0; s < (int)ls->matrix_clusters.size(); ++s) {
+        LightSlice::SamplingRecord &record = ls->sampling_records[s];
+        record.start = true;
+        record.w = Vec3(0.0f);
+        record.f = 0.0f;
+        record.sum_f = record.sum_vpl;
+    }
+    h->metro_ready = true;
+}
+
+/* LightSlice::eval_incoming_radiance(slice[i], xy[i]) (FIXED_RADIUS). */
+void rref_ls_density(void *hp, const int32_t *slice, const float *xy, int n, float *out) {
+    RefLs *h = (RefLs *)hp;
+    metro_prepare(h);
+    for (int i = 0; i < n; ++i) {
+        Vec2 x(xy[2 * i], xy[2 * i + 1]);
+        out[i] = h->ls->eval_incoming_radiance(slice[i], x);
+    }
+}
+
+/* Selects the direction sampler of rref_ls_guided: 0 JENSEN, 1 METROPOLIS (whose chains
+ * then start afresh). */
+void rref_ls_set_sampler(void *hp, int sampler) {
+    RefLs *h = (RefLs *)hp;
+    h->sampler = sampler;
+    if (sampler == 1) {
+        if (h->metro_ready) {
+            for (size_t s = 0; s < h->ls->sampling_records.size(); ++s) {
+                h->ls->sampling_records[s].start = true;
+                h->ls->slices[s].sample_remains = 0;
+            }
+        }
+        metro_prepare(h);
+    }
+}
+
 /* Guided path tracing of the given pixels (VirtualPointLight::guided_path_trace,
  * vpl.cc:907-932, pixel-centre rays): sample s of pixel k from the stream
  * (seed, 6, k * spp + s); out[(i * spp + s) * 3] for the i-th listed pixel. */
@@ -497,7 +561,7 @@ void rref_ls_guided(void *hp, const int32_t *pixels, int n, int spp, int max_bou
                     int direct, uint32_t seed, float *out) {
     RefLs *h = (RefLs *)hp;
     LightSlice *ls = h->ls;
-    ls->sampling_type = LightSlice::LocalSampler::JENSEN;
+    ls->sampling_type = h->sampler == 1 ? LightSlice::LocalSampler::METROPOLIS : LightSlice::LocalSampler::JENSEN;
     Scene *scene = ls->scene;
     Size2 img = scene->get_image_size();
     for (int i = 0; i < n; ++i) {

@@ -21,6 +21,19 @@ struct GuideDev {
     const float *row_cdf;     // [slice][res]
     const float *col_cdf;     // [slice][res][res]
     const float *total;       // [slice]: DiscretePdf2D dist_total
+    // Metropolis sampler (lightslice.cc:1427-1517, 1709-1928)
+    const int *m_off;         // [slice + 1]: the slice's points
+    const int *m_cell;        // [slice][m_grid^2 + 1]: first point of each cell (row-major)
+    int m_grid;               // cells per side of the unit square
+    const float2 *m_pt;       // per point: visible cluster direction on the record's unit square
+    const float4 *m_rad;      // per point: cluster weight x R(slice, representative)
+    const float *sum_f;       // [slice]: SamplingRecord sum_f = sum_vpl (estimate_sum)
+    const int *c_off;         // [slice + 1]: the slice's clusters
+    const float *c_cdf;       // per cluster: the slice's cluster distribution (CDF)
+    const float *c_wi;        // per cluster [3]: direction to its representative
+    const float4 *pool;       // [slice][pool_n]: chain states (direction, density)
+    int pool_n;
+    float density_radius;
     int n_kd, n_slices, res;
     float view_cos;           // cos(pi / 4) as the host computes it (view_similarity_cosine_max)
     float diag;               // scene box diagonal (map_vec6)
@@ -351,6 +364,91 @@ __device__ __forceinline__ Rgb guide_sample_at(const GuideDev &G, const GuideRec
     }
     wi = l2w(r.uvn, w2l(rec, ws));   // same local direction at the receiver
     pdf = guide_pdf_at(G, r, s, wi);
+    return brdf_eval(m, r.uvn, r.wo, wi);
+}
+
+// LightSlice::eval_incoming_radiance with FIXED_RADIUS (lightslice.cc:1427-1517): the
+// radiance of the slice's points strictly within density_radius of x on the unit square
+// (KdTree2::find_nearest with a radius, kdtree_2.cc:203-234, finds exactly these), its
+// luminance (Rgb::luminance, the norm, rgb.h:57) plus density_epsilon_ratio (1e-2) x sum_vpl
+// The cells a query at (x, y) reads: rows [*y0, *y1], columns [*x0, *x1] of the grid, padded
+// by a little so that rounding of (x +- r) * grid never drops a cell holding a point within r
+// (the distance test decides membership).
+__device__ __forceinline__ void guide_cells(const GuideDev &G, float x, float y, int &x0, int &x1, int &y0,
+                                            int &y1) {
+    const float r = G.density_radius, n = (float)G.m_grid;
+    x0 = max(0, (int)floorf((x - r) * n - 1e-3f));
+    x1 = min(G.m_grid - 1, (int)floorf((x + r) * n + 1e-3f));
+    y0 = max(0, (int)floorf((y - r) * n - 1e-3f));
+    y1 = min(G.m_grid - 1, (int)floorf((y + r) * n + 1e-3f));
+}
+
+__device__ __forceinline__ float guide_density(const GuideDev &G, int s, float x, float y) {
+    const float r2 = G.density_radius * G.density_radius;
+    float sr = 0.0f, sg = 0.0f, sb = 0.0f;
+    int x0, x1, y0, y1;
+    guide_cells(G, x, y, x0, x1, y0, y1);
+    const int *cell = G.m_cell + (size_t)s * (G.m_grid * G.m_grid + 1);
+    for (int cy = y0; cy <= y1; ++cy) {
+        for (int i = cell[cy * G.m_grid + x0], e = cell[cy * G.m_grid + x1 + 1]; i < e; ++i) {
+            const float2 q = G.m_pt[i];
+            const float dx = q.x - x, dy = q.y - y;
+            if (dx * dx + dy * dy < r2) {
+                const float4 c = G.m_rad[i];
+                sr += c.x;
+                sg += c.y;
+                sb += c.z;
+            }
+        }
+    }
+    return 1e-2f * G.sum_f[s] + sqrtf(sr * sr + sg * sg + sb * sb);
+}
+
+// LightSlice::metropolis_get_pdf (lightslice.cc:1913-1928) at a world direction
+__device__ __forceinline__ float guide_metro_pdf_map(const GuideDev &G, int s, V3 dir) {
+    const V3 lw = w2l(guide_rec_onb(G, s), dir);
+    if (lw.z <= 0.0f) return 0.0f;
+    const float sum = G.sum_f[s];
+    if (!(sum > 0.0f)) return 0.0f;
+    float sx, sy;
+    guide_direction_to_square(lw, sx, sy);
+    return guide_density(G, s, sx, sy) / sum;
+}
+
+// LightSlice::multi_slice_pdf (lightslice.cc:1930-2056) with the METROPOLIS sampler
+__device__ __forceinline__ float guide_metro_pdf_at(const GuideDev &G, const GuideRecv &r, int s, V3 wi) {
+    if (r.mat < 0) return 0.0f;
+    if (dot(r.ns, wi) <= 0.0f) return 0.0f;
+    if (s < 0) return INV_2PI;
+    const V3 dir = l2w(guide_rec_onb(G, s), w2l(r.uvn, wi));
+    return guide_metro_pdf_map(G, s, dir);
+}
+
+// LightSlice::multi_slice_sample (lightslice.cc:1569-1707) with metropolis_fetch_cached_sample
+// (lightslice.cc:1709-1761): a state of the slice's chain, drawn uniformly from the pool the
+// chain kernel filled (the reference hands out its 1,024-state caches in shuffled order);
+// the pdf is the density over sum_f, not the chain's.  Returns the receiver's BRDF.
+__device__ __forceinline__ Rgb guide_metro_sample_at(const GuideDev &G, const GuideRecv &r, const rzk_material &m,
+                                                     int s, Rng &g, V3 &wi, float &pdf) {
+    if (r.mat < 0) {
+        wi = mk(0.0f, 0.0f, 0.0f);
+        pdf = 0.0f;
+        return crgb(0.0f, 0.0f, 0.0f);
+    }
+    if (s < 0) {   // no usable record: uniform hemisphere at the receiver
+        const float sx = g.uniform(), sy = g.uniform();
+        const float phi = TWO_PI * sx;
+        const float theta = acosf(sy);
+        wi = unit(guide_spherical(r.uvn, theta, phi));
+        pdf = INV_2PI;
+        return brdf_eval(m, r.uvn, r.wo, wi);
+    }
+    int k = (int)(g.uniform() * G.pool_n);
+    if (k >= G.pool_n) k = G.pool_n - 1;
+    const float4 st = G.pool[(size_t)s * G.pool_n + k];
+    const V3 ws = mk(st.x, st.y, st.z);
+    wi = l2w(r.uvn, w2l(guide_rec_onb(G, s), ws));   // same local direction at the receiver
+    pdf = guide_metro_pdf_at(G, r, s, wi);
     return brdf_eval(m, r.uvn, r.wo, wi);
 }
 

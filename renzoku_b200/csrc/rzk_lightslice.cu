@@ -654,6 +654,18 @@ struct rzk_lightslice {
     std::vector<float> map_cdf_col;             // [slice][res][res]
     std::vector<float> map_row_pdf, map_row_cdf;   // [slice][res]
     std::vector<float> map_total;               // [slice]
+    // Metropolis sampler: per slice its visible clusters' directions on the unit square of the
+    // slice's sampling record and their radiance weight x R(slice, representative) (the
+    // points of the slice's KdTree2, lightslice.cc:1182-1217), and the cluster distribution's
+    // CDF and directions (the chain's first state)
+    std::vector<int> m_off;                     // [slice + 1] point offsets
+    std::vector<float> m_pt;                    // [point][2], a slice's points ordered by grid cell
+    std::vector<float> m_rad;                   // [point][4]: r, g, b, 0
+    std::vector<int> m_cell;                    // [slice][grid^2 + 1]: first point of each cell
+    int m_grid = 1;                             // cells per side, each at least density_radius wide
+    std::vector<int> c_off;                     // [slice + 1] cluster offsets
+    std::vector<float> c_cdf;                   // [cluster]
+    std::vector<float> c_wi;                    // [cluster][3]
     std::vector<int> vpl1_orig;                 // one-bounce VPL -> input VPL index
     std::vector<rzk_receiver> rep_recv;         // per slice
     std::vector<int4> h_kd;                     // upper tree for the device lookup
@@ -671,6 +683,8 @@ struct rzk_lightslice {
     bool guide_ready = false;
     DBuf<float> g_box, g_rep, g_uvn, g_prob, g_row_cdf, g_col_cdf, g_total;
     DBuf<uint8_t> g_valid;
+    DBuf<int> g_m_off, g_m_cell, g_c_off;
+    DBuf<float> g_m_pt, g_m_rad, g_c_cdf, g_c_wi, g_sum;
     // per-gather scratch (grown on demand)
     DBuf<int> d_slice, d_count, d_off, d_cursor, d_pix, d_tile_off, d_order, d_vis_off, d_work;
     DBuf<long long> d_mask_off;
@@ -767,6 +781,31 @@ void slice_points(rzk_lightslice *L, const float *h_pts, const int *h_pix, int n
     L->n_kd = (int)L->h_kd.size();
 }
 
+// orders slice s's Metropolis points by the grid cell they fall in (row-major, stable) and
+// appends the slice's cell offsets, so that a density query reads only the cells within
+// density_radius of it
+void bin_points(rzk_lightslice *L, int s) {
+    const int G = L->m_grid, b = L->m_off[s], e = L->m_off[s + 1];
+    std::vector<int> cell(e - b), count(G * G + 1, 0);
+    for (int i = b; i < e; ++i) {
+        const int cx = std::min(G - 1, std::max(0, (int)(L->m_pt[2 * (size_t)i] * G)));
+        const int cy = std::min(G - 1, std::max(0, (int)(L->m_pt[2 * (size_t)i + 1] * G)));
+        cell[i - b] = cy * G + cx;
+        count[cell[i - b] + 1]++;
+    }
+    for (int c = 0; c < G * G; ++c) count[c + 1] += count[c];
+    std::vector<float> pt(2 * (size_t)(e - b)), rad(4 * (size_t)(e - b));
+    std::vector<int> cursor(count.begin(), count.end() - 1);
+    for (int i = b; i < e; ++i) {
+        const int to = cursor[cell[i - b]]++;
+        std::copy(&L->m_pt[2 * (size_t)i], &L->m_pt[2 * (size_t)i] + 2, &pt[2 * (size_t)to]);
+        std::copy(&L->m_rad[4 * (size_t)i], &L->m_rad[4 * (size_t)i] + 4, &rad[4 * (size_t)to]);
+    }
+    std::copy(pt.begin(), pt.end(), L->m_pt.begin() + 2 * (size_t)b);
+    std::copy(rad.begin(), rad.end(), L->m_rad.begin() + 4 * (size_t)b);
+    for (int c = 0; c <= G * G; ++c) L->m_cell.push_back(b + count[c]);
+}
+
 // phase D: per-slice refinement, totals and cluster distribution (in parallel over slices),
 // validity and Jensen's maps.  hR / hV: the reduced matrix and visibility, column-major
 // [n1][ns]; global: the clusters of ClusterBuilder::cluster_by_sampling.
@@ -846,10 +885,16 @@ void refine_slices(rzk_lightslice *L, const float *hR, const uint8_t *hV, int n1
         for (auto &t : th) t.join();
     }
     L->cluster_pdf.clear();
+    L->c_off.assign(1, 0);
+    L->c_cdf.clear();
+    L->c_wi.clear();
     for (int s = 0; s < ns; ++s) {
         DPdf d;
         d.set(cpdf[s].data(), (int)cpdf[s].size());
         L->cluster_pdf.insert(L->cluster_pdf.end(), d.pdf.begin(), d.pdf.end());
+        L->c_cdf.insert(L->c_cdf.end(), d.cdf.begin(), d.cdf.end());
+        for (const HostCluster &c : L->clusters[s]) L->c_wi.insert(L->c_wi.end(), c.wi, c.wi + 3);
+        L->c_off.push_back((int)L->c_cdf.size());
     }
     L->ms[4] = now_ms() - t0;
 
@@ -863,6 +908,11 @@ void refine_slices(rzk_lightslice *L, const float *hR, const uint8_t *hV, int n1
     L->map_row_pdf.assign((size_t)ns * res, 0.0f);
     L->map_row_cdf.assign((size_t)ns * res, 0.0f);
     L->map_total.assign(ns, 0.0f);
+    L->m_off.assign(1, 0);
+    L->m_pt.clear();
+    L->m_rad.clear();
+    L->m_cell.clear();
+    L->m_grid = std::max(1, std::min(64, (int)(1.0f / P.density_radius)));
     for (int s = 0; s < ns; ++s) {
         const std::vector<HostCluster> &cl = L->clusters[s];
         float tot[3] = {0.0f, 0.0f, 0.0f};
@@ -899,10 +949,15 @@ void refine_slices(rzk_lightslice *L, const float *hR, const uint8_t *hV, int n1
                 const float lum = std::sqrt(rr * rr + rg * rg + rb * rb);
                 map[(size_t)iy * res + ix] += lum;
                 msum += lum;
+                L->m_pt.push_back(sx);
+                L->m_pt.push_back(sy);
+                L->m_rad.insert(L->m_rad.end(), {rr, rg, rb, 0.0f});
             }
             for (int j = 0; j < res; ++j)
                 for (int i = 0; i < res; ++i) map[(size_t)i * res + j] += P.map_epsilon * msum;
         }
+        L->m_off.push_back((int)(L->m_pt.size() / 2));
+        bin_points(L, s);
         // DiscretePdf2D::set_distribution (pdf.cc:195-229)
         std::vector<float> row_sum(res);
         float total = 0.0f;
@@ -1130,6 +1185,26 @@ rzk_status rzk::guide_tables(rzk_lightslice *L, GuideDev *out, cudaStream_t st) 
                                cudaMemcpyHostToDevice, st));
         LS_TRY(cudaMemcpyAsync(L->g_total.p, L->map_total.data(), sizeof(float) * ns, cudaMemcpyHostToDevice, st));
         LS_TRY(cudaMemcpyAsync(L->g_valid.p, L->valid.data(), ns, cudaMemcpyHostToDevice, st));
+        // Metropolis tables (one element at least, so that every pointer is valid)
+        auto up_i = [&](DBuf<int> &d, const std::vector<int> &h) -> rzk_status {
+            LS_TRY(d.alloc(std::max<size_t>(1, h.size())));
+            if (!h.empty()) LS_TRY(cudaMemcpyAsync(d.p, h.data(), sizeof(int) * h.size(), cudaMemcpyHostToDevice, st));
+            return RZK_OK;
+        };
+        auto up_f = [&](DBuf<float> &d, const std::vector<float> &h) -> rzk_status {
+            LS_TRY(d.alloc(std::max<size_t>(1, h.size())));
+            if (!h.empty()) LS_TRY(cudaMemcpyAsync(d.p, h.data(), sizeof(float) * h.size(), cudaMemcpyHostToDevice, st));
+            return RZK_OK;
+        };
+        rzk_status r;
+        if ((r = up_i(L->g_m_off, L->m_off)) != RZK_OK) return r;
+        if ((r = up_i(L->g_m_cell, L->m_cell)) != RZK_OK) return r;
+        if ((r = up_i(L->g_c_off, L->c_off)) != RZK_OK) return r;
+        if ((r = up_f(L->g_m_pt, L->m_pt)) != RZK_OK) return r;
+        if ((r = up_f(L->g_m_rad, L->m_rad)) != RZK_OK) return r;
+        if ((r = up_f(L->g_c_cdf, L->c_cdf)) != RZK_OK) return r;
+        if ((r = up_f(L->g_c_wi, L->c_wi)) != RZK_OK) return r;
+        if ((r = up_f(L->g_sum, L->sum_vpl)) != RZK_OK) return r;
         LS_TRY(cudaStreamSynchronize(st));
         L->guide_ready = true;
     }
@@ -1143,6 +1218,18 @@ rzk_status rzk::guide_tables(rzk_lightslice *L, GuideDev *out, cudaStream_t st) 
     G.row_cdf = L->g_row_cdf.p;
     G.col_cdf = L->g_col_cdf.p;
     G.total = L->g_total.p;
+    G.m_off = L->g_m_off.p;
+    G.m_cell = L->g_m_cell.p;
+    G.m_grid = L->m_grid;
+    G.m_pt = reinterpret_cast<const float2 *>(L->g_m_pt.p);
+    G.m_rad = reinterpret_cast<const float4 *>(L->g_m_rad.p);
+    G.sum_f = L->g_sum.p;
+    G.c_off = L->g_c_off.p;
+    G.c_cdf = L->g_c_cdf.p;
+    G.c_wi = L->g_c_wi.p;
+    G.density_radius = L->prm.density_radius;
+    G.pool = nullptr;
+    G.pool_n = 0;
     G.n_kd = L->n_kd;
     G.n_slices = ns;
     G.res = res;

@@ -104,6 +104,8 @@ SIGNATURES = [
     ("rzk_lightslice_host_find", I32, [P, P, I32, P]),
     ("rzk_lightslice_gather", I32, [P, P, I32, I32, F32, F32, P, P]),
     ("rzk_guided_render", I32, [P, P, P, P, P, P, P, P]),
+    ("rzk_lightslice_density", I32, [P, P, P, I32, P, P]),
+    ("rzk_lightslice_chains", I32, [P, U32, I32, P, P]),
     ("rzk_server_create", I32, [I32, P, P]),
     ("rzk_server_destroy", I32, [P]),
     ("rzk_server_submit", I32, [P, P, P]),
@@ -697,7 +699,11 @@ def lightslice_params(**kw) -> LightSliceParamsC:
 class GuidedParamsC(ctypes.Structure):
     """ctypes mirror of rzk_guided_params."""
     _fields_ = [("spp", I32), ("max_bounce", I32), ("rr_depth", I32), ("rr_prob", F32),
-                ("direct_lighting", I32), ("seed", U32)]
+                ("direct_lighting", I32), ("seed", U32), ("sampler", I32), ("chain_samples", I32)]
+
+
+GUIDE_JENSEN = 0
+GUIDE_METROPOLIS = 1
 
 
 class LightSliceCuda:
@@ -826,19 +832,42 @@ class LightSliceCuda:
         return out
 
     def guided_render(self, cam: "Camera", spp: int, max_bounce: int, rr_depth: int = 0, rr_prob: float = 1.0,
-                      direct: bool = True, seed: int = 2013, paths: bool = False, out=None, stream=None):
-        """LightSlice-guided path tracing (rzk_guided_render): the per-pixel mean image, and the
-        per-path radiance [W*H, spp, 3] when paths=True."""
+                      direct: bool = True, seed: int = 2013, paths: bool = False, out=None, stream=None,
+                      sampler: str = "jensen", chain_samples: int = 0):
+        """LightSlice-guided path tracing (rzk_guided_render) with the "jensen" or "metropolis"
+        direction sampler: the per-pixel mean image, and the per-path radiance [W*H, spp, 3]
+        when paths=True."""
         torch = _torch()
         n = cam.n_pixels
         if out is None:
             out = torch.empty((n, 3), dtype=torch.float32, device="cuda")
         pt = torch.empty((n, spp, 3), dtype=torch.float32, device="cuda") if paths else None
-        prm = GuidedParamsC(spp, max_bounce, rr_depth, rr_prob, 1 if direct else 0, seed)
+        mode = {"jensen": GUIDE_JENSEN, "metropolis": GUIDE_METROPOLIS}[sampler]
+        prm = GuidedParamsC(spp, max_bounce, rr_depth, rr_prob, 1 if direct else 0, seed, mode, chain_samples)
         check(self.lib.rzk_guided_render(self.agg.ctx.h, self.agg.h, self.h, cam.rec.ctypes.data, ctypes.byref(prm),
                                          _dptr(out), _dptr(pt) if pt is not None else None, _stream_ptr(stream)),
               "rzk_guided_render")
         return (out, pt) if paths else out
+
+    def density(self, slices, xy, stream=None):
+        """The METROPOLIS sampler's density (rzk_lightslice_density): eval_incoming_radiance of
+        slices[i] at the unit-square point xy[i]; a float32 tensor [n] on the device."""
+        torch = _torch()
+        sl = torch.as_tensor(np.ascontiguousarray(slices, np.int32), device="cuda")
+        pts = torch.as_tensor(np.ascontiguousarray(xy, np.float32).reshape(-1, 2), device="cuda")
+        out = torch.empty(sl.shape[0], dtype=torch.float32, device="cuda")
+        check(self.lib.rzk_lightslice_density(self.h, _dptr(sl), _dptr(pts), int(sl.shape[0]), _dptr(out),
+                                              _stream_ptr(stream)), "rzk_lightslice_density")
+        return out
+
+    def chains(self, seed: int, n_samples: int, stream=None):
+        """The METROPOLIS chains (rzk_lightslice_chains): [n_slices, n_samples, 4] states after
+        the warm-up as (unit-square x, y, density, 0), on the device."""
+        torch = _torch()
+        out = torch.empty((self.info()["slices"], n_samples, 4), dtype=torch.float32, device="cuda")
+        check(self.lib.rzk_lightslice_chains(self.h, seed, n_samples, _dptr(out), _stream_ptr(stream)),
+              "rzk_lightslice_chains")
+        return out
 
     def close(self):
         if getattr(self, "h", None):
