@@ -573,6 +573,7 @@ typedef struct {
     float rr_prob;
     uint32_t seed;
     float *d_rgb;                 /* caller-owned device output, width * height * 3 floats */
+    int32_t sampler;              /* guided: RZK_GUIDE_JENSEN (0) or RZK_GUIDE_METROPOLIS (1) */
 } rzk_request;
 
 typedef struct {

@@ -124,9 +124,9 @@ void launch_group(rzk_server *s, Group *g) {
     for (Req *q : live) {
         const rzk_request &r = q->r;
         if (r.kind == RZK_REQ_GUIDED) {
-            rzk_guided_params gp{r.spp, r.max_bounce, r.rr_depth, r.rr_prob, 1, r.seed};
+            rzk_guided_params gp{r.spp, r.max_bounce, r.rr_depth, r.rr_prob, 1, r.seed, r.sampler, 0};
             q->status = rzk_guided_render(s->ctx, r.scene, r.lightslice, &r.camera, &gp, r.d_rgb, nullptr, st);
-            g->launches += 2;   // path kernel + per-pixel mean
+            g->launches += r.sampler == RZK_GUIDE_METROPOLIS ? 3 : 2;   // (chains +) path kernel + per-pixel mean
         } else if (!s->prm.batching) {
             q->status = rzk_gather_cfg(s->ctx, r.scene, q->d_recv, r.camera.width * r.camera.height, r.camera.width,
                                        r.d_vpls, r.n_vpl, r.clamp_mode, r.tau, r.scale, r.d_rgb, 0, 0, st);
@@ -297,7 +297,8 @@ rzk_status rzk_server_submit(rzk_server *s, const rzk_request *req, uint64_t *ti
             bytes += sizeof(rzk_vpl) * (size_t)r.n_vpl + rzk::order_scratch_bytes(r.n_vpl);
     } else if (r.kind == RZK_REQ_GUIDED) {
         if (!r.lightslice || r.spp <= 0 || r.max_bounce < 1 || r.max_bounce > 16 || r.rr_depth < 0 ||
-            (r.rr_depth > 0 && !(r.rr_prob > 0.0f && r.rr_prob <= 1.0f)))
+            (r.rr_depth > 0 && !(r.rr_prob > 0.0f && r.rr_prob <= 1.0f)) ||
+            (r.sampler != RZK_GUIDE_JENSEN && r.sampler != RZK_GUIDE_METROPOLIS))
             return RZK_ERR_INVALID;
     } else {
         return RZK_ERR_INVALID;

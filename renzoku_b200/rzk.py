@@ -894,7 +894,8 @@ class RequestC(ctypes.Structure):
     """ctypes mirror of rzk_request."""
     _fields_ = [("kind", I32), ("scene", P), ("lightslice", P), ("camera", CameraC), ("d_vpls", P),
                 ("n_vpl", I32), ("clamp_mode", I32), ("tau", F32), ("scale", F32), ("spp", I32),
-                ("max_bounce", I32), ("rr_depth", I32), ("rr_prob", F32), ("seed", U32), ("d_rgb", P)]
+                ("max_bounce", I32), ("rr_depth", I32), ("rr_prob", F32), ("seed", U32), ("d_rgb", P),
+                ("sampler", I32)]
 
 
 class ServerParamsC(ctypes.Structure):

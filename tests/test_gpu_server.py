@@ -1,5 +1,5 @@
 """The request loop (rzk_server_*): admitted requests produce the same images as the direct
-calls, in batched and in one-at-a-time mode; admission refuses what does not fit the HBM
+calls (gathers, and guided renders with either sampler), in batched and in one-at-a-time mode; admission refuses what does not fit the HBM
 budget; queued requests can be withdrawn."""
 import numpy as np
 import pytest
@@ -47,6 +47,7 @@ def world(ctx):
         r.tau = 1e-3
         r.scale = 1.0 / 600
         r.spp, r.max_bounce, r.rr_depth, r.rr_prob, r.seed = 2, 4, 2, 0.5, SEED + i
+        r.sampler = rzk.GUIDE_METROPOLIS if (i // 3) % 2 else rzk.GUIDE_JENSEN
         r.d_rgb = out.data_ptr()
         reqs.append({"req": r, "out": out, "cam": cam, "w": w})
     return scenes, reqs
@@ -61,8 +62,9 @@ def _direct(r):
         ev = rzk.VirtualPointLightCuda(w["agg"], q.clamp_mode, q.tau)
         return ev.gather(recv, r["cam"].n_pixels, w["vpls"], q.n_vpl, scale=q.scale,
                          image_width=r["cam"].width).cpu().numpy()
+    sampler = "metropolis" if q.sampler == rzk.GUIDE_METROPOLIS else "jensen"
     return w["ls"].guided_render(r["cam"], q.spp, q.max_bounce, rr_depth=q.rr_depth, rr_prob=q.rr_prob,
-                                 seed=q.seed).cpu().numpy()
+                                 seed=q.seed, sampler=sampler).cpu().numpy()
 
 
 @pytest.mark.parametrize("batching", [True, False])
