@@ -358,3 +358,27 @@ def test_null_leaves_keys_without_values(tmp_path):
     scene, cam, info, facts = _compare(path)
     white = scene.mats["kd"] == np.array([0.125, 0.25, 0.375], np.float32)
     assert white.all(axis=1).sum() == 1 and cam is not None
+
+
+def test_escapes_and_number_forms_match_reference(tmp_path):
+    """Names written with \\u escapes (a surrogate pair included) bind to the same names
+    written as raw UTF-8; integers, exponents and -0 read as the reference reads them
+    (atoi for integers, atof then float for the rest)."""
+    from renzoku_b200 import rzk
+    doc = _scene_doc()
+    text = json.dumps(doc, ensure_ascii=False)
+    text = text.replace('"white": {"type": "lambertian", "kd": [0.75, 0.75, 0.7]}',
+                        '"wh\\u00eete\\ud83d\\ude00": {"type": "lambertian", "kd": [7.5E-1, 75e-2, -0]}')
+    text = text.replace('"unnamed": {"mesh": "room", "bsdf": "white"}',
+                        '"unnamed": {"mesh": "room", "bsdf": "whîte\U0001F600"}')
+    text = text.replace('"stale": {"mesh": "coloured", "bsdf": "white"}',
+                        '"stale": {"mesh": "coloured", "bsdf": "wh\\u00eete\\ud83d\\ude00"}')
+    text = text.replace('"bsdf": "white"', '"bsdf": "whîte😀"')
+    assert "white" not in text
+    path = _write_tree(tmp_path, None, text)
+    scene, cam, info, facts = _compare(path)
+    kd = np.array([0.75, 0.75, 0.0], np.float32)
+    assert (scene.mats["kd"] == kd).all(axis=1).sum() == 1
+    (tmp_path / "plain").mkdir()
+    _, _, base = rzk.import_json(str(_write_tree(tmp_path / "plain", _scene_doc())))
+    assert info["n_prims"] == base["n_prims"] and info["skipped"] == base["skipped"]
