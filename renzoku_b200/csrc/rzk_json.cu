@@ -480,10 +480,27 @@ struct Importer {
         if (options) {
             if (const JVal *g = get(*options, "geometry")) {
                 const JVal &geo = as_object(*g);
+                if (has(geo, "traversal")) (void)as_string(need(get(geo, "traversal"), "traversal"));
                 if (has(geo, "tmin")) info.tmin = as_numeric(need(get(geo, "tmin"), "tmin"));
                 if (has(geo, "two_sided_surfaces"))
                     info.two_sided = as_bool(need(get(geo, "two_sided_surfaces"), "two_sided_surfaces")) ? 1 : 0;
             }
+            // the OpenGL viewer's options are read (and required where the reference requires
+            // them) though nothing here uses them (json_importer.cc:810-829)
+            if (const JVal *o = get(*options, "opengl")) {
+                const JVal &gl = as_object(*o);
+                if (const JVal *v = get(gl, "shadow_map")) {
+                    const JVal &sm = as_object(*v);
+                    (void)as_numeric(strict(sm, "polygon_offset_factor"));
+                    (void)as_numeric(strict(sm, "polygon_offset_unit"));
+                }
+                if (const JVal *v = get(gl, "sensor")) {
+                    const JVal &so = as_object(*v);
+                    (void)as_string(strict(so, "multi_sample"));
+                    (void)as_int(strict(so, "num_antialiased_samples"));
+                }
+            }
+            if (const JVal *e = get(*options, "experimental")) (void)as_object(*e);
         }
         if (!views.empty()) {
             const View &vw = views[0];

@@ -333,6 +333,17 @@ BAD = [
                          '"views": {}}}'),
     ("null_pairs_past_values", '{"materials": {"a": null, "b": {"type": "lambertian", "kd": [1,1,1]}}}'),
 ]
+_OPT_SCENE = ('{"cameras": {"c": {"type": "pinhole", "pos": [0,0,1], "lookat": [0,0,0], "up": [0,1,0], '
+              '"near": 0.1, "far": 1, "image": [8,8], "film": [1,1], "fov": 40}}, "scene": {"world": '
+              '{"surfaces": {}, "lights": {}}, "views": {"v": {"camera": "c", "integrator": {"type": "vpl", '
+              '"max_bounce": 3, "samples": 1}}}, "options": %s}}')
+BAD += [
+    ("shadow_map_without_factor", _OPT_SCENE % '{"opengl": {"shadow_map": {"polygon_offset_unit": 2}}}'),
+    ("sensor_samples_real", _OPT_SCENE % '{"opengl": {"sensor": {"multi_sample": "msaa", '
+                                         '"num_antialiased_samples": 4.0}}}'),
+    ("traversal_not_string", _OPT_SCENE % '{"geometry": {"traversal": 3}}'),
+    ("experimental_not_object", _OPT_SCENE % '{"experimental": [1, 2]}'),
+]
 
 
 @pytest.mark.parametrize("name,text", BAD, ids=[b[0] for b in BAD])
