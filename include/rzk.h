@@ -176,8 +176,9 @@ typedef struct {
                                                 OBJ material: left out */
     int32_t skipped;                     /* entries the reference reports and skips (unknown
                                             types, names that resolve to nothing) */
-    int32_t faces_with_vertex_normals;   /* summed over the OBJ files (rzk_obj_info) */
-    int32_t smoothed_faces;
+    int32_t faces_with_vertex_normals;   /* imported faces given vertex normals, and faces in a */
+    int32_t smoothed_faces;              /* smoothing group without them: facet normals here,
+                                            interpolated shading normals in the reference */
 } rzk_json_info;
 
 /* Reads `path` and the OBJ and MTL files it names.  RZK_ERR_INVALID where the reference stops

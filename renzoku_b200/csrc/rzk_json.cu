@@ -105,6 +105,7 @@ struct Shape {
     int kind = 0;
     float v[12] = {0};
     int surface = -1;   // Shape::surface_index
+    int shading = 0;    // ObjShape::shading
 };
 enum { S_MATERIAL, S_LIGHT, S_UNSUPPORTED, S_SPHERE };
 struct Surf {
@@ -171,8 +172,6 @@ struct Importer {
         const std::string path = scene_path + "mesh/" + file;
         if (rzk::obj_load(path.c_str(), m) != RZK_OK) throw Fail("cannot read " + path);
         info.obj_files++;
-        info.faces_with_vertex_normals += m.info.faces_with_vertex_normals;
-        info.smoothed_faces += m.info.smoothed_faces;
         const int base = (int)shapes.size();
         for (const rzk::ObjShape &s : m.shapes) {
             Shape sh;
@@ -180,6 +179,7 @@ struct Importer {
             sh.kind = s.kind;
             std::memcpy(sh.v, s.v, sizeof(sh.v));
             sh.surface = s.surface;   // the OBJ importer's own surface index
+            sh.shading = s.shading;
             shapes.push_back(sh);
         }
         return base;
@@ -523,6 +523,10 @@ struct Importer {
         std::vector<int> scene_mat(mats.size(), -1);
         const int flags = info.two_sided ? RZK_SURF_TWO_SIDED : 0;
         for (const Surf &sf : surfaces) {
+            if ((sf.type == S_MATERIAL || sf.type == S_LIGHT) && sf.shape >= 0) {
+                if (shapes[sf.shape].shading == 1) info.faces_with_vertex_normals++;
+                else if (shapes[sf.shape].shading == 2) info.smoothed_faces++;
+            }
             if (sf.type == S_MATERIAL) {
                 if (scene_mat[sf.mat] < 0) {
                     scene_mat[sf.mat] = (int)out.mats.size();

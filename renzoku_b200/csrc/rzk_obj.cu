@@ -312,6 +312,11 @@ rzk_status obj_load(const char *path, ObjModel &o) {
         put_geometry(fc.count, fc.v, verts, sh.kind, sh.v);
         sh.object = fc.object;
         sh.surface = -1;
+        {
+            bool normals_given = false;
+            for (int k = 0; k < fc.count; ++k) normals_given |= fc.n[k] >= 0;
+            sh.shading = normals_given ? 1 : (fc.smooth > 0 ? 2 : 0);
+        }
         if (fc.mat < 0) {
             info.faces_without_material++;
             o.shapes.push_back(sh);
@@ -340,10 +345,8 @@ rzk_status obj_load(const char *path, ObjModel &o) {
             sf.mat = mat_of[fc.mat];
         }
         if (sf.type != OBJ_SURF_UNSUPPORTED) {
-            bool normals_given = false;
-            for (int k = 0; k < fc.count; ++k) normals_given |= fc.n[k] >= 0;
-            if (normals_given) info.faces_with_vertex_normals++;
-            else if (fc.smooth > 0) info.smoothed_faces++;
+            if (sh.shading == 1) info.faces_with_vertex_normals++;
+            else if (sh.shading == 2) info.smoothed_faces++;
         }
         sh.surface = (int)o.surfaces.size();
         sf.shape = (int)o.shapes.size();

@@ -15,6 +15,8 @@ struct ObjShape {
     float v[12];    // vertices; the fourth is zero for a triangle
     int object;     // index into ObjModel::object_names (the `o` line before it), -1 before any
     int surface;    // the importer's surface index (Surfaces::append, surface.h:123-127), -1 for none
+    int shading;    // 1: vertex normals given, 2: in a smoothing group without them (the
+                    // reference interpolates shading normals; facet normals here), 0: neither
 };
 
 // One entry of the importer's surface list.

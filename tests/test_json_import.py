@@ -108,6 +108,11 @@ o lamp_extra
 f 9 11 10
 o walls
 f 2 6 7
+vn 0 0 1
+o bumpy
+f 2//1 3//1 7//1
+s 2
+f 2 7 6
 """
 
 MESH_PROPS_MTL = """newmtl prop_red
@@ -210,6 +215,7 @@ def _scene_doc():
                     "no_such_bsdf": {"mesh": "room.floor", "bsdf": "nothing"},
                     "obj_material": {"mesh": "room.lamp_extra", "bsdf": "prop_glossy"},
                     "stale": {"mesh": "coloured", "bsdf": "white"},
+                    "bumpy": {"mesh": "room.bumpy", "bsdf": "white"},
                 },
                 "lights": {
                     "top": {"light": "ceiling_light", "mesh": "room.lamp"},
@@ -271,6 +277,8 @@ def test_every_section_matches_reference_importer(tmp_path):
     # the unknown light, a point light bound to a mesh, the unknown camera, the photon view
     assert info["skipped"] == 12
     assert info["n_lights"] == 3   # the OBJ's light quad and emitting face, the lamp
+    # bound faces the reference shades with interpolated normals: counted
+    assert info["faces_with_vertex_normals"] == 1 and info["smoothed_faces"] == 1
 
 
 def test_fov_camera_matches_reference(tmp_path):
