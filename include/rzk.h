@@ -12,8 +12,7 @@
  *     rzk_context).  A context is single-threaded: use one per host thread.
  *
  * Each entry point names the reference interface it replaces (file:line in the
- * reference project).  INTEGRATION.md shows the C++ classes a maintainer adds to the
- * reference tree to bind them.
+ * reference project).
  */
 #ifndef RZK_H_
 #define RZK_H_
@@ -43,6 +42,12 @@ rzk_status rzk_context_destroy(rzk_context *ctx);
 /* Reads and clears the device error word (RZK_OK when no kernel reported a problem).
  * Synchronises `stream`. */
 rzk_status rzk_context_check(rzk_context *ctx, void *stream);
+/* Shadow rays the gather kernels of this context have traced since it was created or last
+ * reset: every (receiver, VPL) pair that survives the exact-zero test (both BRDFs' own
+ * early-outs, lambertian.cc:63-66, phong.cc:74-77, ward.cc:104-109) and so needs
+ * Aggregate::hit(p, q) (aggregate.cc:84-90).  One atomic add per warp work item.  Reads
+ * after `stream` has run; reset != 0 also zeroes the counter on `stream`. */
+rzk_status rzk_context_rays(rzk_context *ctx, uint64_t *h_rays, int reset, void *stream);
 
 /* Aggregate ------------------------------------------------------------------------- */
 
@@ -273,18 +278,26 @@ rzk_status rzk_gather_host(rzk_context *ctx, rzk_scene *scene, const rzk_receive
  * For callers that cannot let the library call cudaMalloc - their device memory is owned
  * by another framework's allocator or held to a fixed budget, or they run a frame loop in
  * which an allocation (which can synchronise the device or fail) is not acceptable.  The
- * scratch (per-VPL-chunk partial sums and a work counter) is a fixed static device array
- * of RZK_NOALLOC_SCRATCH_BYTES (16 MiB) that every GPU loading the library holds until
- * the process exits; the call itself allocates and frees nothing.
- *   - Limit: n_recv * 12 bytes must fit in the array minus 256 bytes (about 1.39 million
- *     receivers); larger requests return RZK_ERR_CAPACITY before any device work.
+ * scratch (a work counter, per-VPL-chunk partial sums and, when it fits, the spatially
+ * ordered VPL copy with its sort scratch) is a fixed static device array of
+ * RZK_NOALLOC_SCRATCH_BYTES (16 MiB) that every GPU loading the library holds until the
+ * process exits; the call itself allocates and frees nothing.
+ *   - Limit: n_recv * 12 bytes (rounded up to 256) must fit in the array minus 256 bytes
+ *     (about 1.39 million receivers); larger requests return RZK_ERR_CAPACITY before any
+ *     device work.
+ *   - The current device must be the scene's context's device (else RZK_ERR_INVALID).
  *   - The first call on a device looks up the array's device address there (once per
  *     device, with that device current); make that first call before any stream capture.
- *   - All calls share the one array, and it keeps the previous call's contents: calls
- *     whose work overlaps on the GPU (other streams, other host threads) race and must
- *     be serialised by the caller.
- *   - Result: the same per-receiver sums as rzk_gather, formed over as many VPL chunks
- *     as fit (at most 32), so the float summation order can differ from rzk_gather's. */
+ *   - All calls share the one array, and it keeps the previous call's contents (the call
+ *     clears what it uses first): calls whose work overlaps on the GPU (other streams,
+ *     other host threads) race and must be serialised by the caller.
+ *   - Result: rzk_gather's chunking (at most 32 chunks of >= 128 VPLs, the VPLs in the
+ *     Hilbert order) wherever its partial sums and the ordered copy fit - then the image is
+ *     rzk_gather's bit for bit; otherwise fewer chunks, or the caller's VPL order, change
+ *     only the float summation order.
+ *   - Like every kernel of the library it reports a bounded wait that gave up in the
+ *     context's error word, not in its return value: check rzk_context_check on the
+ *     scene's context after the stream has run the call. */
 rzk_status rzk_gather_noalloc(rzk_scene *scene, const rzk_receiver *d_recv, int n_recv,
                               int image_width, const rzk_vpl *d_vpls, int n_vpl, int clamp_mode,
                               float tau, float scale, float *d_rgb, void *stream);
@@ -473,6 +486,11 @@ rzk_status rzk_lightslice_slices(const rzk_lightslice *ls, int32_t *h_point_pixe
 rzk_status rzk_lightslice_clusters(const rzk_lightslice *ls, int32_t *h_count, int32_t *h_rep, float *h_weight,
                                    uint8_t *h_upper, float *h_wi, float *h_incident, float *h_pdf,
                                    int32_t *h_size, int32_t *h_members);
+/* The global clustering of the one-bounce VPL columns (ClusterBuilder::cluster_by_sampling,
+ * cluster_builder.cc:82-273, as LightSlice::initialize runs it, lightslice.cc:756-762):
+ * per global cluster (n_global_clusters of rzk_lightslice_info) its representative column
+ * and weight, per column (n_vpl_used) its cluster.  Any pointer may be NULL. */
+rzk_status rzk_lightslice_global(const rzk_lightslice *ls, int32_t *h_rep, float *h_weight, int32_t *h_assign);
 /* Jensen maps [slice][res][res] (row-major, row = y), validity, VPL sum, row CDFs
  * [slice][res] and column CDFs [slice][res][res] (DiscretePdf2D, pdf.cc:195-229). */
 rzk_status rzk_lightslice_maps(const rzk_lightslice *ls, float *h_maps, uint8_t *h_valid, float *h_sum,

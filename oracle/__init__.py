@@ -21,7 +21,9 @@ from renzoku_b200 import scenegen as sg
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "librzk_ref.so")
-REFERENCE_TREE = "/root/reference"
+# the reference source tree, read only to compile _ref/librzk_ref.so (absent where the
+# prebuilt library travels without it)
+REFERENCE_TREE = os.environ.get("RZK_REFERENCE_TREE", "/root/reference")
 
 P = ctypes.c_void_p
 I32 = ctypes.c_int32
@@ -43,7 +45,7 @@ def build(ref: bool = True) -> None:
     targets = ["oracle"]
     if ref and os.path.isdir(REFERENCE_TREE):
         targets.append("ref")
-    subprocess.run(["make", "-s", "-j8", "-C", HERE, *targets], check=True)
+    subprocess.run(["make", "-s", "-j8", "-C", HERE, f"REF={REFERENCE_TREE}", *targets], check=True)
 
 
 def _ptr(a: np.ndarray):
@@ -271,6 +273,8 @@ class RefHarness:
             L.rref_ls_find.argtypes = [P, P, I32, P]
             L.rref_ls_reduced_matrix.restype = I32
             L.rref_ls_reduced_matrix.argtypes = [P, P, I32, I32, F32, P, P, P]
+            L.rref_ls_set_vpls.restype = I32
+            L.rref_ls_set_vpls.argtypes = [P, P, I32]
             L.rref_ls_refine.argtypes = [P, P, P, I32, I32, P, P, P, P, I32, U32, I32, F32, F32]
             L.rref_ls_num_slice_clusters.restype = I32
             L.rref_ls_num_slice_clusters.argtypes = [P]
@@ -509,6 +513,13 @@ class RefLightSlice:
         assert got == n1
         self.n_vpl1 = n1
         return R, V, rep
+
+    def set_vpls(self, vpls):
+        """Loads the one-bounce VPLs without tracing the reduced matrix (for a matrix computed
+        elsewhere and passed to refine)."""
+        vpls = np.ascontiguousarray(vpls)
+        self.n_vpl1 = RefHarness.lib().rref_ls_set_vpls(self.h, _ptr(vpls), len(vpls))
+        return self.n_vpl1
 
     def refine(self, R, V, g_rep, g_weight, assign, mags, max_slice_clusters, seed, res=32, eps=1e-3,
                density_radius=0.1):

@@ -238,6 +238,16 @@ int rref_ls_reduced_matrix(void *hp, const rzk_vpl *vpls, int n_vpl, int inc_mod
     return n1;
 }
 
+/* The one-bounce VPLs of the LightSlice without tracing the reduced matrix (for callers
+ * that pass a reduced matrix computed elsewhere to rref_ls_refine); returns their count. */
+int rref_ls_set_vpls(void *hp, const rzk_vpl *vpls, int n_vpl) {
+    RefLs *h = (RefLs *)hp;
+    h->vpls1.clear();
+    for (int i = 0; i < n_vpl; ++i)
+        if (vpls[i].bounce <= 1) h->vpls1.push_back(to_vpl(h->s, vpls[i]));
+    return (int)h->vpls1.size();
+}
+
 /* Per-slice refinement and maps from the given reduced matrix and global clusters. */
 void rref_ls_refine(void *hp, const float *R, const uint8_t *V, int n1, int n_global, const int32_t *g_rep,
                     const float *g_weight, const int32_t *assign, const float *mags, int max_slice_clusters,

@@ -69,8 +69,10 @@ rzk_status rzk_context_create(int device, rzk_context **out) {
     RZK_CUDA_TRY(cudaSetDevice(device));
     rzk_context *c = new rzk_context();
     c->device = device;
-    cudaError_t e = cudaMalloc((void **)&c->d_err, sizeof(uint32_t));
-    if (e == cudaSuccess) e = cudaMemset(c->d_err, 0, sizeof(uint32_t));
+    // one 16-byte allocation: the error word, then (8-byte aligned) the ray counter
+    cudaError_t e = cudaMalloc((void **)&c->d_err, 16);
+    if (e == cudaSuccess) e = cudaMemset(c->d_err, 0, 16);
+    c->d_rays = (unsigned long long *)((char *)c->d_err + 8);
     if (e != cudaSuccess) {
         set_last_cuda_error(e, "context", __FILE__, __LINE__);
         delete c;
@@ -101,6 +103,16 @@ rzk_status rzk_context_check(rzk_context *c, void *stream) {
     if (w & ERR_TIMEOUT) return RZK_ERR_TIMEOUT;
     if (w & ERR_STACK) return RZK_ERR_STACK;
     if (w) return RZK_ERR_CUDA;
+    return RZK_OK;
+}
+
+rzk_status rzk_context_rays(rzk_context *c, uint64_t *h_rays, int reset, void *stream) {
+    if (!c || !h_rays) return RZK_ERR_INVALID;
+    unsigned long long n = 0;
+    RZK_CUDA_TRY(cudaMemcpyAsync(&n, c->d_rays, sizeof(n), cudaMemcpyDeviceToHost, as_stream(stream)));
+    RZK_CUDA_TRY(cudaStreamSynchronize(as_stream(stream)));
+    if (reset) RZK_CUDA_TRY(cudaMemsetAsync(c->d_rays, 0, sizeof(n), as_stream(stream)));
+    *h_rays = (uint64_t)n;
     return RZK_OK;
 }
 

@@ -15,6 +15,7 @@
 #include "rzk_gather_dev.cuh"
 
 #include <algorithm>
+#include <mutex>
 
 namespace rzk {
 
@@ -828,18 +829,27 @@ rzk_status launch_gather_scratch(const DevScene &s, const rzk_receiver *recv, in
     int chunk_len = n_vpl > 0 ? (n_vpl + n_chunks - 1) / n_chunks : 0;
     chunk_len = (chunk_len + 127) / 128 * 128;
     if (chunk_len > 0) n_chunks = (n_vpl + chunk_len - 1) / chunk_len;
-    static int grid_per_device[64] = {0};
+    // resident grid per device, computed once per device (std::call_once: concurrent first
+    // calls from several host threads wait for the one computation)
+    struct Grid {
+        std::once_flag once;
+        int blocks = 0;
+        cudaError_t err = cudaSuccess;
+    };
+    static Grid grid_per_device[64];
     int dev = 0;
     RZK_CUDA_TRY(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64) return RZK_ERR_UNSUPPORTED;
-    if (grid_per_device[dev] == 0) {
+    Grid &g = grid_per_device[dev];
+    std::call_once(g.once, [&g, dev] {
         int sms = 0, per_sm = 0;
-        RZK_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        RZK_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gather_persistent_kernel<4, 32, 5>,
-                                                                   128, 0));
-        grid_per_device[dev] = std::max(1, sms * std::max(1, per_sm));
-    }
-    gather_persistent_kernel<4, 32, 5><<<grid_per_device[dev], 128, 0, st>>>(
+        g.err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (g.err == cudaSuccess)
+            g.err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gather_persistent_kernel<4, 32, 5>, 128, 0);
+        g.blocks = std::max(1, sms * std::max(1, per_sm));
+    });
+    RZK_CUDA_TRY(g.err);
+    gather_persistent_kernel<4, 32, 5><<<g.blocks, 128, 0, st>>>(
         s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, (int)wtiles, work, mode, tau, partial);
     RZK_CUDA_TRY(cudaGetLastError());
     reduce_chunks_kernel<<<(3 * n_recv + 255) / 256, 256, 0, st>>>(partial, n_recv, n_chunks, scale, out);

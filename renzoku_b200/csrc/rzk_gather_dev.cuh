@@ -323,6 +323,7 @@ __device__ __forceinline__ bool gather_item(const DevScene &s, const rzk_receive
         return true;
     }
     Rgb sum = crgb(0.0f, 0.0f, 0.0f);
+    unsigned long long n_rays = 0;         // shadow rays of this item (lane 0's count)
     int occ_cache = -1, occ_cache2 = -1;   // this lane's last two occluders (any-hit tree leaves)
     if (lane == 0) {
         int cnt = min(TILE, j1 - j0);
@@ -348,7 +349,9 @@ __device__ __forceinline__ bool gather_item(const DevScene &s, const rzk_receive
             const rzk_vpl &l = tile[v];
             PairGeo pg;
             bool act = active && pair_survives(r, l, pg);
-            if (!__any_sync(kFull, act)) continue;
+            const unsigned am = __ballot_sync(kFull, act);
+            if (!am) continue;
+            n_rays += (unsigned)__popc(am);
             Ray ray = make_ray(r.p, sub(pg.q, r.p));
             float tmax = len(sub(pg.q, r.p)) - s.tmin;
             if (packet_visible_near(s, ray, tmax, act, ws.stk, occ_cache, occ_cache2)) {
@@ -357,6 +360,7 @@ __device__ __forceinline__ bool gather_item(const DevScene &s, const rzk_receive
         }
         __syncwarp();
     }
+    if (lane == 0 && s.rays && n_rays) atomicAdd(s.rays, n_rays);
     if (ri >= 0) {
         float *o = partial + 3 * ((size_t)chunk * n_recv + ri);
         o[0] = sum.r; o[1] = sum.g; o[2] = sum.b;
@@ -387,6 +391,7 @@ __device__ __forceinline__ bool visibility_item(const DevScene &s, const rzk_rec
         return true;
     }
     int occ_cache = -1, occ_cache2 = -1;
+    unsigned long long n_rays = 0;
     if (lane == 0) {
         int cnt = min(TILE, j1 - j0);
         fence_proxy_async();
@@ -412,7 +417,9 @@ __device__ __forceinline__ bool visibility_item(const DevScene &s, const rzk_rec
             PairGeo pg;
             bool act = active && pair_survives(r, l, pg);
             unsigned vis = 0u;
-            if (__any_sync(kFull, act)) {
+            const unsigned am = __ballot_sync(kFull, act);
+            n_rays += (unsigned)__popc(am);
+            if (am) {
                 Ray ray = make_ray(r.p, sub(pg.q, r.p));
                 float tmax = len(sub(pg.q, r.p)) - s.tmin;
                 vis = __ballot_sync(kFull, packet_visible_near(s, ray, tmax, act, ws.stk, occ_cache, occ_cache2));
@@ -421,6 +428,7 @@ __device__ __forceinline__ bool visibility_item(const DevScene &s, const rzk_rec
         }
         __syncwarp();
     }
+    if (lane == 0 && s.rays && n_rays) atomicAdd(s.rays, n_rays);
     return true;
 }
 

@@ -53,6 +53,7 @@ struct DevScene {
     int n_tris, n_nodes, n_mats, n_lights;
     float tmin;
     uint32_t *err;            // device error word (context-owned)
+    unsigned long long *rays; // shadow rays traced by the gather kernels (context-owned counter)
 };
 
 struct Scene;
@@ -63,7 +64,8 @@ struct BatchPlan;   // rzk_batch.cu: a batch of gathers split into launch tables
 
 struct rzk_context {
     int device = 0;
-    uint32_t *d_err = nullptr;
+    uint32_t *d_err = nullptr;             // error word (the first 8 bytes of a 16-byte allocation)
+    unsigned long long *d_rays = nullptr;  // shadow rays traced by the gather kernels (its last 8)
     // reusable gather scratch: per-(VPL chunk, receiver) partial sums
     float *d_partial = nullptr;
     size_t partial_bytes = 0;
@@ -121,6 +123,7 @@ struct rzk_scene {
         s.surf = d_surf; s.mats = d_mats; s.lights = d_lights; s.light_pdf = d_light_pdf;
         s.light_cdf = d_light_cdf; s.n_tris = n_tris; s.n_nodes = n_nodes; s.n_mats = n_mats;
         s.n_lights = n_lights; s.tmin = tmin; s.err = ctx ? ctx->d_err : nullptr;
+        s.rays = ctx ? ctx->d_rays : nullptr;
         return s;
     }
 };

@@ -667,6 +667,10 @@ struct rzk_lightslice {
     std::vector<float> c_cdf;                   // [cluster]
     std::vector<float> c_wi;                    // [cluster][3]
     std::vector<int> vpl1_orig;                 // one-bounce VPL -> input VPL index
+    // the global clustering as cluster_by_sampling returned it: per cluster its
+    // representative column and weight, per column its cluster
+    std::vector<int32_t> global_rep, global_assign;
+    std::vector<float> global_weight;
     std::vector<rzk_receiver> rep_recv;         // per slice
     std::vector<int4> h_kd;                     // upper tree for the device lookup
     bool on_device = false;                     // false: built from host inputs, no gather
@@ -1103,6 +1107,9 @@ rzk_status build(rzk_lightslice *L, const rzk_receiver *d_recv, const rzk_vpl *d
             for (int i = 0; i < n1; ++i) { assign[i] = i; rep[i] = i; w[i] = 1.0f; }
         }
         global = make_global(n1, ng, rep.data(), w.data(), assign.data(), mags.data());
+        L->global_rep.assign(rep.begin(), rep.begin() + ng);
+        L->global_weight.assign(w.begin(), w.begin() + ng);
+        L->global_assign = assign;
     }
     L->ms[3] = now_ms() - t0;
 
@@ -1335,6 +1342,14 @@ rzk_status rzk_lightslice_info(const rzk_lightslice *L, int32_t *n_points, int32
         *n_slice_clusters = (int32_t)t;
     }
     if (h_ms) for (int i = 0; i < 8; ++i) h_ms[i] = L->ms[i];
+    return RZK_OK;
+}
+
+rzk_status rzk_lightslice_global(const rzk_lightslice *L, int32_t *h_rep, float *h_weight, int32_t *h_assign) {
+    if (!L || !L->on_device) return RZK_ERR_INVALID;
+    if (h_rep) std::copy(L->global_rep.begin(), L->global_rep.end(), h_rep);
+    if (h_weight) std::copy(L->global_weight.begin(), L->global_weight.end(), h_weight);
+    if (h_assign) std::copy(L->global_assign.begin(), L->global_assign.end(), h_assign);
     return RZK_OK;
 }
 

@@ -42,6 +42,7 @@ SIGNATURES = [
     ("rzk_context_create", I32, [I32, P]),
     ("rzk_context_destroy", I32, [P]),
     ("rzk_context_check", I32, [P, P]),
+    ("rzk_context_rays", I32, [P, P, I32, P]),
     ("rzk_scene_create", I32, [P, P, P, P]),
     ("rzk_scene_destroy", I32, [P]),
     ("rzk_scene_info", I32, [P, P, P, P, P]),
@@ -95,6 +96,7 @@ SIGNATURES = [
     ("rzk_lightslice_destroy", I32, [P]),
     ("rzk_lightslice_info", I32, [P, P, P, P, P, P, P]),
     ("rzk_lightslice_slices", I32, [P, P, P, P, P, P]),
+    ("rzk_lightslice_global", I32, [P, P, P, P]),
     ("rzk_lightslice_clusters", I32, [P, P, P, P, P, P, P, P, P, P]),
     ("rzk_lightslice_maps", I32, [P, P, P, P, P, P]),
     ("rzk_lightslice_matrix", I32, [P, P, P, P, P]),
@@ -185,6 +187,14 @@ class Context:
 
     def check(self, stream=None) -> None:
         check(self.lib.rzk_context_check(self.h, _stream_ptr(stream)), "device error word")
+
+    def rays(self, reset: bool = False, stream=None) -> int:
+        """Shadow rays the gather kernels traced since creation or the last reset
+        (rzk_context_rays)."""
+        n = ctypes.c_uint64()
+        check(self.lib.rzk_context_rays(self.h, ctypes.byref(n), 1 if reset else 0, _stream_ptr(stream)),
+              "rzk_context_rays")
+        return int(n.value)
 
     def close(self):
         if getattr(self, "h", None):
@@ -769,6 +779,17 @@ class LightSliceCuda:
         check(self.lib.rzk_lightslice_slices(self.h, pp.ctypes.data, st.ctypes.data, en.ctypes.data, rp.ctypes.data,
                                              nb.ctypes.data), "rzk_lightslice_slices")
         return {"point_pixel": pp, "start": st, "end": en, "rep": rp, "neighbors": nb}
+
+    def global_clusters(self):
+        """The global clustering (rzk_lightslice_global): representatives, weights and each
+        one-bounce column's cluster."""
+        inf = self.info()
+        rep = np.zeros(inf["global_clusters"], np.int32)
+        w = np.zeros(inf["global_clusters"], np.float32)
+        assign = np.zeros(inf["vpls_used"], np.int32)
+        check(self.lib.rzk_lightslice_global(self.h, rep.ctypes.data, w.ctypes.data, assign.ctypes.data),
+              "rzk_lightslice_global")
+        return rep, w, assign
 
     def clusters(self):
         inf = self.info()

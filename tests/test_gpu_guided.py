@@ -58,6 +58,8 @@ def test_guided_paths_match_reference(ctx, oracle_built, rr_depth):
     ours = paths[pix]
     scale = np.maximum(np.abs(ref).max(axis=2), 1e-3)
     close = (np.abs(ours - ref).max(axis=2) <= 1e-4 * scale + 1e-6)
+    rel = float(np.linalg.norm(ours.mean(axis=1) - ref.mean(axis=1)) / np.linalg.norm(ref.mean(axis=1)))
+    print(f"PARITY guided32 rr{rr_depth}: paths agreeing {close.mean():.5f}, image rel-L2 {rel:.3e}")
     assert close.mean() > 0.95, close.mean()
     m_ref, m_ours = ref.mean(axis=(0, 1)), ours.mean(axis=(0, 1))
     assert np.allclose(m_ours, m_ref, rtol=0.02), (m_ours, m_ref)
