@@ -92,6 +92,14 @@ rzk_status rzk_occluded_batch(rzk_scene *scene, const float *d_p, const float *d
 rzk_status rzk_closest_batch(rzk_scene *scene, const float *d_o, const float *d_d, int n,
                              float *d_t, rzk_receiver *d_recv, void *stream);
 
+/* AggregateBvh::hit for n rays given as constructed reference Rays with their own
+ * [tmin, tmax] (no re-normalisation: the query sees the caller's Ray bit for bit):
+ * closest = 0 is the any-hit query hit(ray, tmin, tmax, time) (aggregate_bvh.cc:452-478);
+ * closest = 1 is hit(ray, tmin, tmax, time, HitRecord&) (aggregate_bvh.cc:402-448) up
+ * to the record fill, returning what that fill starts from (t, beta, gamma, triangle). */
+rzk_status rzk_ray_query_batch(rzk_scene *scene, const rzk_ray *d_rays, int n, int closest,
+                               rzk_ray_hit *d_out, void *stream);
+
 /* One pixel-centre primary hit per pixel: Camera::shoot_ray(i, j) (camera.cc:52-65)
  * then the closest hit; row-major, row 0 at the top of the image.  `h_cam` is a host
  * struct (use rzk_camera_setup). d_out has width*height receivers. */
@@ -158,7 +166,10 @@ rzk_status rzk_obj_destroy(rzk_obj *obj);
  * path does not model is counted and left out; the scene equals the reference's where those
  * counts are 0. */
 typedef struct rzk_json rzk_json;
-enum { RZK_JSON_NONE = 0, RZK_JSON_PATH = 1, RZK_JSON_VPL = 2 };
+enum { RZK_JSON_NONE = 0, RZK_JSON_PATH = 1, RZK_JSON_VPL = 2, RZK_JSON_VPL_CUDA = 3 };
+/* options.geometry.traversal (json_importer.cc:857-883): "bvh" (also the default and what an
+ * unknown name reverts to), "none", and this library's "cuda_lbvh". */
+enum { RZK_TRAVERSAL_BVH = 0, RZK_TRAVERSAL_NONE = 1, RZK_TRAVERSAL_CUDA_LBVH = 2 };
 typedef struct {
     int32_t n_prims, n_mats, n_lights;   /* the scene description's primitives, materials,
                                             area lights */
@@ -169,7 +180,9 @@ typedef struct {
     int32_t width, height;               /* "image" */
     float film_w, film_h;                /* "film" */
     float near_plane, far_plane;
-    int32_t integrator;                  /* that view's integrator: RZK_JSON_PATH or _VPL */
+    int32_t integrator;                  /* that view's integrator: RZK_JSON_PATH, _VPL, or
+                                            _VPL_CUDA ("vpl_cuda": this library's gather,
+                                            which the reference's load_integrator lacks) */
     int32_t max_bounce, samples;
     float tmin;                          /* options.geometry.tmin, else RAY_TMIN (1e-3) */
     int32_t two_sided;                   /* options.geometry.two_sided_surfaces: every
@@ -184,6 +197,7 @@ typedef struct {
     int32_t faces_with_vertex_normals;   /* imported faces given vertex normals, and faces in a */
     int32_t smoothed_faces;              /* smoothing group without them: facet normals here,
                                             interpolated shading normals in the reference */
+    int32_t traversal;                   /* RZK_TRAVERSAL_* from options.geometry.traversal */
 } rzk_json_info;
 
 /* Reads `path` and the OBJ and MTL files it names.  RZK_ERR_INVALID where the reference stops

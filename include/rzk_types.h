@@ -113,6 +113,25 @@ typedef struct {
     int32_t pad;
 } rzk_camera;
 
+/* One ray exactly as a constructed reference Ray holds it (ray.h:17-36: origin, unit
+ * direction, inverse direction after the ZERO_EPSILON substitution, -origin x inverse
+ * direction) and the interval [tmin, tmax] of the query: 16 words.                  */
+typedef struct {
+    float o[3], d[3], inv_d[3], org_inv_d[3];
+    float tmin, tmax;
+    int32_t pad[2];
+} rzk_ray;
+
+/* Result of one ray query: 8 words.  hit = 1 when a triangle passes; for closest-hit
+ * queries also the reference's GeometryHit (t, beta, gamma; triangle.cc:158-232) and the
+ * hit triangle's index in the flattened order of rzk_scene.h (else -1).            */
+typedef struct {
+    int32_t hit;
+    float t, beta, gamma;
+    int32_t tri;
+    int32_t pad[3];
+} rzk_ray_hit;
+
 /* Flat BVH node as the reference numbers it (BvhNode, aggregate_bvh.h:10-16):
  * used only for dumps and bit-exact comparison.                                 */
 typedef struct {

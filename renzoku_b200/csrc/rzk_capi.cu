@@ -19,6 +19,8 @@ void set_last_cuda_error(cudaError_t e, const char *what, const char *file, int 
 
 rzk_status launch_occluded(const DevScene &s, const float *p, const float *q, int n, uint8_t *out,
                            cudaStream_t st);
+rzk_status launch_ray_query(const DevScene &s, const int *perm, const rzk_ray *rays, int n, int closest,
+                            rzk_ray_hit *out, cudaStream_t st);
 rzk_status launch_closest(const DevScene &s, const float *o, const float *d, int n, float *t,
                           rzk_receiver *recv, cudaStream_t st);
 rzk_status launch_primary(const DevScene &s, const rzk_camera &cam, rzk_receiver *out, cudaStream_t st);
@@ -278,6 +280,13 @@ rzk_status rzk_closest_batch(rzk_scene *s, const float *d_o, const float *d_d, i
     if (!s || n < 0 || (n > 0 && (!d_o || !d_d))) return RZK_ERR_INVALID;
     if (d_recv && !aligned16(d_recv)) return RZK_ERR_INVALID;
     return launch_closest(s->dev(), d_o, d_d, n, d_t, d_recv, as_stream(stream));
+}
+
+rzk_status rzk_ray_query_batch(rzk_scene *s, const rzk_ray *d_rays, int n, int closest, rzk_ray_hit *d_out,
+                               void *stream) {
+    if (!s || n < 0 || (closest != 0 && closest != 1) || (n > 0 && (!d_rays || !d_out))) return RZK_ERR_INVALID;
+    if (n > 0 && (!aligned16(d_rays) || !aligned16(d_out))) return RZK_ERR_INVALID;
+    return launch_ray_query(s->dev(), s->d_perm, d_rays, n, closest, d_out, as_stream(stream));
 }
 
 rzk_status rzk_primary(rzk_scene *s, const rzk_camera *cam, rzk_receiver *d_out, void *stream) {

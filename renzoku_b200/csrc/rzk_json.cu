@@ -362,9 +362,11 @@ struct Importer {
             View vw;
             vw.max_bounce = as_int(need(get(spec, "max_bounce"), "max_bounce"));
             const std::string type = as_string(need(get(spec, "type"), "type"));
-            if (type != "path" && type != "vpl") { info.skipped++; continue; }
+            // "vpl_cuda" is this library's extension of the seam: the device gather, read with
+            // the keys of "vpl"
+            if (type != "path" && type != "vpl" && type != "vpl_cuda") { info.skipped++; continue; }
             vw.samples = as_int(need(get(spec, "samples"), "samples"));
-            vw.integrator = type == "path" ? RZK_JSON_PATH : RZK_JSON_VPL;
+            vw.integrator = type == "path" ? RZK_JSON_PATH : type == "vpl" ? RZK_JSON_VPL : RZK_JSON_VPL_CUDA;
             vw.camera = camera_index(as_string(need(get(view, "camera"), "camera")));
             if (vw.camera < 0) { info.skipped++; continue; }
             views.push_back(vw);
@@ -480,7 +482,13 @@ struct Importer {
         if (options) {
             if (const JVal *g = get(*options, "geometry")) {
                 const JVal &geo = as_object(*g);
-                if (has(geo, "traversal")) (void)as_string(need(get(geo, "traversal"), "traversal"));
+                if (has(geo, "traversal")) {
+                    // json_importer.cc:862-876: "bvh", "none", anything else reverts to BVH;
+                    // "cuda_lbvh" selects this library's device LBVH
+                    const std::string t = as_string(need(get(geo, "traversal"), "traversal"));
+                    info.traversal = t == "none" ? RZK_TRAVERSAL_NONE
+                                   : t == "cuda_lbvh" ? RZK_TRAVERSAL_CUDA_LBVH : RZK_TRAVERSAL_BVH;
+                }
                 if (has(geo, "tmin")) info.tmin = as_numeric(need(get(geo, "tmin"), "tmin"));
                 if (has(geo, "two_sided_surfaces"))
                     info.two_sided = as_bool(need(get(geo, "two_sided_surfaces"), "two_sided_surfaces")) ? 1 : 0;

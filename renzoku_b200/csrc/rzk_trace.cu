@@ -47,6 +47,40 @@ __global__ void __launch_bounds__(kTraceBlock) closest_kernel(DevScene s, const 
     }
 }
 
+// Queries on rays the caller constructed (the reference's Ray fields, its own interval):
+// the caller's ray is used as stored.  Any-hit walks the any-hit tree (same answer, see
+// rzk_sah.cu); closest-hit walks the reference tree in the reference's visit order, which
+// decides ties.
+__global__ void __launch_bounds__(kTraceBlock) ray_query_kernel(DevScene s, const int *perm, const rzk_ray *rays,
+                                                                int n, int closest, rzk_ray_hit *out) {
+    __shared__ int stack_mem[STACK_CAP * kTraceBlock];
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Stack<kTraceBlock> stk;
+    stk.init(stack_mem + threadIdx.x);
+    const rzk_ray &q = rays[i];
+    Ray r;
+    r.o = ld3(q.o);
+    r.d = ld3(q.d);
+    r.inv_d = ld3(q.inv_d);
+    r.org_inv_d = ld3(q.org_inv_d);
+    rzk_ray_hit h{0, 0.0f, 0.0f, 0.0f, -1, {0, 0, 0}};
+    if (closest) {
+        float t, b, g;
+        const int slot = closest_hit<kTraceBlock>(s, r, q.tmin, q.tmax, stk, &t, &b, &g);
+        if (slot >= 0) {
+            h.hit = 1;
+            h.t = t;
+            h.beta = b;
+            h.gamma = g;
+            h.tri = perm[slot];
+        }
+    } else {
+        h.hit = any_hit<kTraceBlock, false, true>(s, r, q.tmin, q.tmax, stk) ? 1 : 0;
+    }
+    out[i] = h;
+}
+
 // One thread per pixel; a block covers an 16 x 8 pixel tile so that a warp's primary
 // rays are spatially coherent.
 __global__ void __launch_bounds__(kTraceBlock) primary_kernel(DevScene s, rzk_camera cam,
@@ -81,6 +115,14 @@ rzk_status launch_closest(const DevScene &s, const float *o, const float *d, int
                           rzk_receiver *recv, cudaStream_t st) {
     if (n <= 0) return RZK_OK;
     closest_kernel<<<(n + kTraceBlock - 1) / kTraceBlock, kTraceBlock, 0, st>>>(s, o, d, n, t, recv);
+    RZK_CUDA_TRY(cudaGetLastError());
+    return RZK_OK;
+}
+
+rzk_status launch_ray_query(const DevScene &s, const int *perm, const rzk_ray *rays, int n, int closest,
+                            rzk_ray_hit *out, cudaStream_t st) {
+    if (n <= 0) return RZK_OK;
+    ray_query_kernel<<<(n + kTraceBlock - 1) / kTraceBlock, kTraceBlock, 0, st>>>(s, perm, rays, n, closest, out);
     RZK_CUDA_TRY(cudaGetLastError());
     return RZK_OK;
 }

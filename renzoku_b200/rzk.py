@@ -58,6 +58,7 @@ SIGNATURES = [
     ("rzk_morton_codes", I32, [P, P, P]),
     ("rzk_occluded_batch", I32, [P, P, P, I32, P, P]),
     ("rzk_closest_batch", I32, [P, P, P, I32, P, P, P]),
+    ("rzk_ray_query_batch", I32, [P, P, I32, I32, P, P]),
     ("rzk_primary", I32, [P, P, P, P]),
     ("rzk_camera_setup", I32, [P, P, P, F32, I32, I32, F32, F32, P]),
     ("rzk_camera_setup_focal", I32, [P, P, P, F32, I32, I32, F32, F32, P]),

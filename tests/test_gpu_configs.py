@@ -73,7 +73,7 @@ def test_config1_full_image_matches_reference(ctx, oracle_built):
     hit = recv["mat"] >= 0
     want = np.zeros((cam.n_pixels, 3), np.float32)
     want[hit] = ref.gather_mt(recv[hit].copy(), vpls, rzk.CLAMP_RADIANCE, tau, scale)
-    assert want.sum() > 0 and hit.sum() > 0.9 * cam.n_pixels
+    assert want.sum() > 0 and hit.sum() > 0.5 * cam.n_pixels
     # one chunk: the reference's summation order, bit for bit, every pixel
     assert np.array_equal(one, want), np.abs(one - want).max()
     assert not one[~hit].any() and not chunked[~hit].any()

@@ -70,11 +70,19 @@ def test_noalloc_matches_oracle(ctx, scene):
     assert np.linalg.norm(got - want) <= 1e-5 * np.linalg.norm(want)
     assert np.linalg.norm(got - want64) <= 1e-5 * np.linalg.norm(want64)
     assert np.all(np.abs(got - want) <= 1e-4 * np.abs(want) + 1e-7)
-    # one chunk (at most 128 VPLs): the oracle's order exactly
-    out1 = torch.empty_like(out)
-    assert _noalloc(lib, agg, recv, cam.n_pixels, 96, vt, 100, rzk.CLAMP_RADIANCE, 0.05, 1.0, out1) == rzk.OK
-    want1, _ = Oracle(sc).gather(recv_np, vpls[:100].copy(), rzk.CLAMP_RADIANCE, 0.05, 1.0)
-    assert np.array_equal(out1.cpu().numpy(), want1)
+    # one chunk (at most 128 VPLs) on an all-Lambertian scene (no transcendental on the
+    # path): the oracle's order and values exactly
+    lam = sg.room_boxes(32, 32)
+    agg1 = rzk.AggregateCuda(ctx, lam)
+    recv1 = agg1.primary(rzk.Camera(lam.camera))
+    vt1, n1 = rzk.VplGeneratorCuda(agg1).spawn(43, 80, 3)
+    n1 = min(n1, 100)
+    out1 = torch.empty((32 * 32, 3), dtype=torch.float32, device="cuda")
+    assert _noalloc(lib, agg1, recv1, 32 * 32, 32, vt1, n1, rzk.CLAMP_RADIANCE, 0.05, 1.0, out1) == rzk.OK
+    want1, _ = Oracle(lam).gather(rzk.records_from_device(recv1, sg.RECEIVER_DTYPE),
+                                  rzk.records_from_device(vt1, sg.VPL_DTYPE)[:n1].copy(), rzk.CLAMP_RADIANCE,
+                                  0.05, 1.0)
+    assert want1.sum() > 0 and np.array_equal(out1.cpu().numpy(), want1)
 
 
 def test_noalloc_smaller_call_after_larger(ctx, scene):
