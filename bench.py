@@ -306,6 +306,7 @@ def run_ours(args):
         step()
     torch.cuda.synchronize()
     ctx.check()
+    ctx.rays(reset=True)   # the device's shadow-ray counter covers the timed steps only
     if pg:
         pg.barrier()
     torch.cuda.synchronize()
@@ -325,6 +326,7 @@ def run_ours(args):
         pg.barrier()
     total = max_over_ranks(pg, sum(times), "cuda")
     ctx.check()
+    rays_timed = ctx.rays(reset=True)
     evals_step = n_recv * N_VPL
     value = job_rate(ws, evals_step, len(times), total)
     launches_step = kernels_per_call(step)
@@ -386,7 +388,7 @@ def run_ours(args):
             peak_src = "measured"
         else:
             peak, peak_src = 6650.0, "fallback"
-        rays_per_eval = cnt["rays"] / pairs
+        rays_per_eval_oracle = cnt["rays"] / pairs
         # CPU baseline: the reference's own gather on this box's host cores, bounded sample
         threads = os.cpu_count() or 1
         if args.skip_cpu:   # profiling runs: the GPU part only
@@ -401,8 +403,12 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": ws, "steps": len(times),
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": workload_config(),
-            "rays_per_s": value * rays_per_eval,
-            "shadow_rays_per_eval": rays_per_eval,
+            "rays_per_s": ws * rays_timed / total,
+            "rays_note": ("shadow rays counted on the device by the gather kernels over the timed steps "
+                          "(rzk_context_rays), over the timed region"),
+            "shadow_rays_per_step": rays_timed / len(times),
+            "shadow_rays_per_eval": rays_timed / len(times) / evals_step,
+            "shadow_rays_per_eval_oracle_sample": rays_per_eval_oracle,
             "e2e": {"value": ws * evals_step / e2e_s, "unit": "evals/s",
                     "h2d_bytes_per_step": n_recv * 96 + N_VPL * 96,
                     "d2h_bytes_per_step": n_recv * 12, "image_finite": img_ok},

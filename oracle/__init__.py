@@ -41,10 +41,13 @@ class Counters(ctypes.Structure):
 
 
 def build(ref: bool = True) -> None:
-    """Compile liboracle.so and, where the reference tree exists, _ref/librzk_ref.so."""
+    """Compile liboracle.so and, where the reference tree exists, _ref/librzk_ref.so and the
+    drop-in classes' driver _ref/librzk_dropin_test.so."""
     targets = ["oracle"]
     if ref and os.path.isdir(REFERENCE_TREE):
         targets.append("ref")
+        if os.path.exists(os.path.join(HERE, "..", "renzoku_b200", "librzk_dropin.so")):
+            targets.append("dropin")
     subprocess.run(["make", "-s", "-j8", "-C", HERE, f"REF={REFERENCE_TREE}", *targets], check=True)
 
 
@@ -582,6 +585,79 @@ class RefLightSlice:
         RefHarness.lib().rref_ls_guided(self.h, _ptr(pixels), len(pixels), spp, max_bounce, rr_depth, rr_prob,
                                         1 if direct else 0, seed, _ptr(out))
         return out
+
+class DropinHarness:
+    """A scene file loaded by the drop-in factory (load_scene_cuda) and driven through the
+    reference's interfaces, beside the reference's AggregateBvh (see ref/dropin_harness.cc)."""
+
+    _lib = None
+    SO = os.path.join(HERE, "_ref", "librzk_dropin_test.so")
+
+    @classmethod
+    def available(cls) -> bool:
+        return os.path.exists(cls.SO) and RefHarness.available()
+
+    @classmethod
+    def lib(cls):
+        if cls._lib is None:
+            RefHarness.lib()
+            L = ctypes.CDLL(cls.SO, mode=ctypes.RTLD_GLOBAL)
+            L.rdi_load.restype = P
+            L.rdi_load.argtypes = [ctypes.c_char_p, I32]
+            L.rdi_kinds.restype = I32
+            L.rdi_kinds.argtypes = [P]
+            L.rdi_segments.restype = I32
+            L.rdi_segments.argtypes = [P, P, P, I32, P, P, P]
+            L.rdi_closest.restype = I32
+            L.rdi_closest.argtypes = [P, P, P, I32, P]
+            L.rdi_vpls.restype = I32
+            L.rdi_vpls.argtypes = [P, U32, I32, I32, P, P, P, P, I32]
+            L.rdi_render.restype = I32
+            L.rdi_render.argtypes = [P, I32, I32, U32, P, I32, P]
+            cls._lib = L
+        return cls._lib
+
+    def __init__(self, path: str, device: int = 0):
+        self.h = self.lib().rdi_load(str(path).encode(), device)
+        if not self.h:
+            raise RuntimeError(f"load_scene_cuda failed on {path}")
+
+    def kinds(self):
+        k = self.lib().rdi_kinds(self.h)
+        return {"aggregate_cuda": bool(k & 1), "integrator_cuda": bool(k & 2)}
+
+    def segments(self, p, q):
+        p = np.ascontiguousarray(p, np.float32)
+        q = np.ascontiguousarray(q, np.float32)
+        n = len(p)
+        virt, batch, ref = (np.zeros(n, np.uint8) for _ in range(3))
+        assert self.lib().rdi_segments(self.h, _ptr(p), _ptr(q), n, _ptr(virt), _ptr(batch), _ptr(ref)) == 0
+        return virt, batch, ref
+
+    def closest(self, o, d):
+        o = np.ascontiguousarray(o, np.float32)
+        d = np.ascontiguousarray(d, np.float32)
+        rec = np.zeros((len(o), 2, 14), np.float32)
+        assert self.lib().rdi_closest(self.h, _ptr(o), _ptr(d), len(o), _ptr(rec)) == 0
+        return rec[:, 0], rec[:, 1]
+
+    def vpls(self, seed, particles, max_bounce, cap=None):
+        cap = cap or particles * max(1, max_bounce - 1)
+        p, c = np.zeros((cap, 3), np.float32), np.zeros((cap, 3), np.float32)
+        b, pv = np.zeros(cap, np.int32), np.zeros(cap, np.int32)
+        n = self.lib().rdi_vpls(self.h, seed, particles, max_bounce, _ptr(p), _ptr(c), _ptr(b), _ptr(pv), cap)
+        assert n >= 0
+        n = min(n, cap)
+        return {"p": p[:n], "contrib": c[:n], "bounce": b[:n], "prev": pv[:n]}
+
+    def render(self, start_particles, max_vpls, seed, width, height):
+        img = np.zeros((height * width, 3), np.float32)
+        info = np.zeros(5, np.float32)
+        st = self.lib().rdi_render(self.h, start_particles, max_vpls, seed, _ptr(img), img.size, _ptr(info))
+        assert st == 0, st
+        return img, {"width": int(info[0]), "height": int(info[1]), "vpls": int(info[2]),
+                     "emitted": int(info[3]), "tau": float(info[4])}
+
 
 def column_magnitudes(mat: np.ndarray) -> np.ndarray:
     """The magnitude of every flattened column [cols][rows][3] summed in order, as

@@ -17,6 +17,10 @@ import sys
 from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+# the reference source tree, read only for its headers by the drop-in classes (absent where
+# the prebuilt librzk_dropin.so travels without it)
+REFERENCE_TREE = os.environ.get("RZK_REFERENCE_TREE", "/root/reference")
+DROPIN = os.path.join(HERE, "librzk_dropin.so")
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "librzk_cuda.so")
 OBJ = os.path.join(HERE, "_build")
@@ -71,5 +75,19 @@ def build(force: bool = False, verbose: bool = False) -> str:
     return LIB
 
 
+def build_dropin(force: bool = False) -> str | None:
+    """librzk_dropin.so (renzoku_b200/dropin): the C++ classes behind the reference's
+    Aggregate / IVplGenerator / Integrator interfaces.  Needs the reference's headers; where
+    they are absent the prebuilt library is used as it is (None if there is none)."""
+    build()
+    if os.path.isdir(REFERENCE_TREE):
+        args = ["make", "-s", "-C", os.path.join(HERE, "dropin"), f"REF={REFERENCE_TREE}"]
+        if force:
+            args.append("-B")
+        subprocess.run(args, check=True)
+    return DROPIN if os.path.exists(DROPIN) else None
+
+
 if __name__ == "__main__":
     build(force="--force" in sys.argv, verbose=True)
+    build_dropin(force="--force" in sys.argv)

@@ -1,5 +1,6 @@
-/* Test-infrastructure shim: declaration-only stand-ins for FreeImage.  The oracle never
- * loads image files; these exist so the reference image header compiles. */
+/* Build stand-in for FreeImage, which this image lacks: declarations only, so that the
+ * reference's image.h compiles.  Nothing built here loads or writes image files; a build
+ * inside the reference's own tree uses the real library instead. */
 #pragma once
 typedef unsigned char BYTE;
 struct FIBITMAP;

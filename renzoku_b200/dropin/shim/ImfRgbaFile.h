@@ -1,5 +1,5 @@
-/* Test-infrastructure shim: declaration-only stand-ins for the OpenEXR types that the
- * reference image header names.  The oracle never writes EXR files. */
+/* Build stand-in for OpenEXR, which this image lacks: declarations of the types the
+ * reference's image.h names.  Nothing built here writes EXR files. */
 #pragma once
 namespace Imf {
 struct Rgba { Rgba() {} Rgba(float, float, float, float) {} };

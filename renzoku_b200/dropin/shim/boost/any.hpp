@@ -1,4 +1,4 @@
-/* Test-infrastructure shim: boost::any mapped onto std::any (C++17). */
+/* Build stand-in for Boost, which this image lacks: boost::any mapped onto std::any. */
 #pragma once
 #include <any>
 namespace boost {

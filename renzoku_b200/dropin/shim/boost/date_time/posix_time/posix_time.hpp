@@ -1,5 +1,5 @@
-/* Test-infrastructure shim: the reference's log timestamps only need a printable
- * time.  No Boost is installed; this replaces ptime/microsec_clock with a stub. */
+/* Build stand-in for Boost, which this image lacks: the reference's log timestamps only
+ * need a printable time, so ptime / microsec_clock are stubs. */
 #pragma once
 #include <string>
 namespace boost { namespace posix_time {

@@ -308,10 +308,11 @@ class JsonInfoC(ctypes.Structure):
                 ("samples", I32), ("tmin", F32), ("two_sided", I32), ("obj_files", I32),
                 ("point_lights", I32), ("spot_lights", I32), ("directional_lights", I32), ("spheres", I32),
                 ("surfaces_unsupported_material", I32), ("skipped", I32), ("faces_with_vertex_normals", I32),
-                ("smoothed_faces", I32)]
+                ("smoothed_faces", I32), ("traversal", I32)]
 
 
-JSON_INTEGRATORS = {0: None, 1: "path", 2: "vpl"}
+JSON_INTEGRATORS = {0: None, 1: "path", 2: "vpl", 3: "vpl_cuda"}
+JSON_TRAVERSALS = {0: "bvh", 1: "none", 2: "cuda_lbvh"}
 
 
 def import_json(path: str):

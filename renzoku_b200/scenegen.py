@@ -372,14 +372,15 @@ def write_obj(scene: Scene, path: str) -> None:
 
 
 def write_json(scene: Scene, path: str, integrator: str = "vpl", max_bounce: int = 3, samples: int = 1,
-               tmin=None, two_sided=None) -> None:
+               tmin=None, two_sided=None, traversal: str = "bvh") -> None:
     """Writes `scene` as a scene file in the reference's JSON format (json_importer.cc) with
     its geometry in one OBJ file without materials (mesh/<name>.obj beside it, one `o` object
     per material, `m<i>`, and per emitter, `e<k>`), which rzk_json_import reads back:
     materials `mat_<i>` (lambertian kd; phong kd, ks, n; ward kd, ks, ax, ay), area light
     specs `area_<k>` with each emitter's radiance, world surfaces binding `<name>.m<i>` to
     `mat_<i>`, world lights binding `<name>.e<k>` to `area_<k>`, a pinhole camera from the
-    scene's camera (fov) and one view with the given integrator.  Reals are written with 9
+    scene's camera (fov), one view with the given integrator and the given
+    options.geometry.traversal ("bvh", "none" or this library's "cuda_lbvh").  Reals are written with 9
     significant digits, so float32 values read back unchanged; the surfaces come back grouped
     by material, then the emitters."""
     import json
@@ -431,7 +432,7 @@ def write_json(scene: Scene, path: str, integrator: str = "vpl", max_bounce: int
             },
             "views": {"main": {"camera": "cam", "integrator": {"type": integrator, "max_bounce": int(max_bounce),
                                                                "samples": int(samples)}}},
-            "options": {"geometry": {"traversal": "bvh"}},
+            "options": {"geometry": {"traversal": traversal}},
         },
     }
     geo = doc["scene"]["options"]["geometry"]
