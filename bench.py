@@ -486,6 +486,28 @@ def run_ours(args):
             "scene": {"triangles": agg.n_tris, "nodes": agg.n_nodes, "levels": agg.n_levels,
                       "device_bytes": agg.device_bytes},
         }
+    if line is not None and ws == 1 and args.serve_duration > 0 and not args.skip_cpu:
+        # the metric's second half: serving latency and throughput, batched server beside the
+        # one-request-at-a-time server, on the serving mix (its own device-resident worlds)
+        del flush
+        torch.cuda.empty_cache()
+        t0 = time.perf_counter()
+        worlds = serve_setup(ctx)
+        setup_s = time.perf_counter() - t0
+        rates = [float(x) for x in SERVE_RATES.split(",")]
+        sweep = serve_sweep(worlds, rates, args.serve_duration, args.budget_gb)
+        keys = ("completed", "rejected", "throughput_rps", "evals_per_s", "paths_per_s", "p50_ms", "p95_ms",
+                "p99_ms", "mean_queue_ms", "mean_run_ms")
+        line["serving"] = {
+            "workload": "serving_mix_8_scenes_50k_1M_tris", "duration_s_per_rate": args.serve_duration,
+            "hbm_budget_gb": args.budget_gb, "setup_s": setup_s,
+            "scene_triangles": [w["agg"].n_tris for w in worlds],
+            "rates": [{"rate_rps": x["rate_rps"], "requests": x["requests"],
+                       "batched": {k: x["batched"][k] for k in keys}, "plain": {k: x["plain"][k] for k in keys},
+                       "evals_per_s_ratio": x["evals_per_s_ratio"], "p99_ratio": x["p99_ratio"]} for x in sweep],
+            "note": ("Poisson arrivals at each rate; latency = the server's submit-to-completion time; the "
+                     "one-request-at-a-time server is the plain per-request path on the same resident scenes"),
+        }
     if pg:
         pg.barrier()
         pg.destroy_process_group()
@@ -867,24 +889,17 @@ def run_guided(args):
     return 0
 
 
-def run_serve(args):
-    """Serving mix: 8 device-resident scenes (room filled to 50k-1M triangles, log-uniform,
-    seed 7), each with 100,000 VPLs and a LightSlice; Poisson arrivals (seed 8) at each rate
-    for --duration seconds; every request is a gather or a guided render (50/50) with image
-    side 64-1024, 1k-100k VPLs and 1-16 spp, log-uniform.  The same request streams run
-    through the batched server and through the one-request-at-a-time server; admission by
-    an HBM budget.  Prints one JSON line (value = p99 latency of the batched server at the
-    lowest rate)."""
-    import dataclasses
+SERVE_RATES = "5,10,20,50,100,200"
+
+
+def serve_setup(ctx):
+    """The serving mix's device-resident worlds: 8 rooms filled to 50k-1M triangles
+    (log-uniform, seed 7), each with 100,000 VPLs, its clamp threshold and a LightSlice."""
     import math
     import torch
-    from renzoku_b200 import build as rbuild
-    rbuild.build()
     from renzoku_b200 import instances as im, rzk, scenegen as sg
-    ctx = rzk.Context(0)
     rng = np.random.default_rng(7)
     worlds = []
-    t0 = time.perf_counter()
     for k in range(8):
         n_tris = int(round(math.exp(rng.uniform(math.log(50_000), math.log(1_000_000)))))
         sc = sg.room_filled(n_tris, 256, 256, 700 + k)
@@ -901,8 +916,21 @@ def run_serve(args):
                                                              seed=VPL_SEED))
         worlds.append({"sc": sc, "agg": agg, "vpls": vt, "emitted": emitted, "tau": tau, "ls": ls})
     torch.cuda.synchronize()
-    setup_s = time.perf_counter() - t0
-    rates = [float(x) for x in args.rates.split(",")]
+    ctx.check()
+    return worlds
+
+
+def serve_sweep(worlds, rates, duration, budget_gb):
+    """Poisson arrivals (seed 8 + rate) at each rate for `duration` seconds; every request a
+    gather or a guided render (50/50) with image side 64-1024, 1k-100k VPLs and 1-16 spp,
+    log-uniform, against one of the worlds.  The same request stream runs through the
+    batched server and through the one-request-at-a-time server.  Latency is the server's
+    submit-to-completion time; throughput counts completed work over the wall time of
+    arrivals plus drain."""
+    import dataclasses
+    import math
+    import torch
+    from renzoku_b200 import rzk
     logu = lambda g, lo, hi: math.exp(g.uniform(math.log(lo), math.log(hi)))
 
     def requests(rate):
@@ -910,7 +938,7 @@ def run_serve(args):
         t, out = 0.0, []
         while True:
             t += g.exponential(1.0 / rate)
-            if t > args.duration:
+            if t > duration:
                 return out
             side = max(64, int(round(logu(g, 64, 1024) / 8.0)) * 8)
             out.append({"t": t, "guided": bool(g.random() < 0.5), "scene": int(g.integers(8)), "side": side,
@@ -933,9 +961,12 @@ def run_serve(args):
         r.d_rgb = out.data_ptr()
         return r
 
+    def pct(x, q):
+        return float(np.percentile(x, q)) if len(x) else None
+
     def run(batching, reqs):
-        srv = rzk.Server(0, batching=batching, hbm_budget_bytes=int(args.budget_gb * (1 << 30)))
-        pending, lat, rejected = {}, [], 0
+        srv = rzk.Server(0, batching=batching, hbm_budget_bytes=int(budget_gb * (1 << 30)))
+        pending, done, rejected = {}, [], 0
         t_start = time.perf_counter()
         for d in reqs:
             while True:
@@ -948,29 +979,57 @@ def run_serve(args):
             if t is None:
                 rejected += 1
             else:
-                pending[t] = out
+                pending[t] = (out, d)
             for tk in list(pending):
                 st, l, _ = srv.poll(tk)
                 if st >= 2:
-                    lat.append(l)
+                    done.append((l, pending[tk][1]))
                     del pending[tk]
         for tk in list(pending):
             _, l = srv.wait(tk)
-            lat.append(l)
+            done.append((l, pending[tk][1]))
         wall = time.perf_counter() - t_start
         stats = srv.stats()
+        kind, q_ms, r_ms = srv.timings()
         srv.close()
-        lat = np.array(lat) if lat else np.zeros(1)
-        return {"completed": len(lat), "rejected": rejected, "wall_s": wall, "throughput_rps": len(lat) / wall,
-                "p50_ms": float(np.percentile(lat, 50)), "p95_ms": float(np.percentile(lat, 95)),
-                "p99_ms": float(np.percentile(lat, 99)), "launches": stats["launches"]}
+        lat = np.array([l for l, _ in done])
+        lat_g = np.array([l for l, d in done if not d["guided"]])
+        lat_p = np.array([l for l, d in done if d["guided"]])
+        evals = sum(d["side"] * d["side"] * d["vpls"] for _, d in done if not d["guided"])
+        paths = sum(d["side"] * d["side"] * d["spp"] for _, d in done if d["guided"])
+        return {"completed": len(done), "rejected": rejected, "wall_s": wall,
+                "throughput_rps": len(done) / wall, "evals_per_s": evals / wall, "paths_per_s": paths / wall,
+                "p50_ms": pct(lat, 50), "p95_ms": pct(lat, 95), "p99_ms": pct(lat, 99),
+                "gather_p99_ms": pct(lat_g, 99), "guided_p99_ms": pct(lat_p, 99),
+                "mean_queue_ms": float(q_ms.mean()) if len(q_ms) else None,
+                "mean_run_ms": float(r_ms.mean()) if len(r_ms) else None,
+                "launches": stats["launches"]}
 
     sweep = []
     for rate in rates:
         reqs = requests(rate)
         b = run(True, reqs)
         p = run(False, reqs)
-        sweep.append({"rate_rps": rate, "requests": len(reqs), "batched": b, "plain": p})
+        sweep.append({"rate_rps": rate, "requests": len(reqs), "batched": b, "plain": p,
+                      "evals_per_s_ratio": b["evals_per_s"] / p["evals_per_s"] if p["evals_per_s"] else None,
+                      "p99_ratio": b["p99_ms"] / p["p99_ms"] if b["p99_ms"] and p["p99_ms"] else None})
+    return sweep
+
+
+def run_serve(args):
+    """Serving mix (see serve_sweep) at the --rates for --duration seconds each, batched
+    server beside the one-request-at-a-time server.  Prints one JSON line (value = p99
+    latency of the batched server at the lowest rate)."""
+    import torch
+    from renzoku_b200 import build as rbuild
+    rbuild.build()
+    from renzoku_b200 import rzk
+    ctx = rzk.Context(0)
+    t0 = time.perf_counter()
+    worlds = serve_setup(ctx)
+    setup_s = time.perf_counter() - t0
+    rates = [float(x) for x in args.rates.split(",")]
+    sweep = serve_sweep(worlds, rates, args.duration, args.budget_gb)
     first = sweep[0]["batched"]
     line = {
         "metric": f"serving p99 latency (ms) at {rates[0]:g} req/s, batched server",
@@ -1006,8 +1065,11 @@ def main():
     ap.add_argument("--side", type=int, default=1024)
     ap.add_argument("--max-slice-clusters", type=int, default=4096)
     ap.add_argument("--slice-size", type=int, default=4096)
-    ap.add_argument("--rates", default="5,20,50,200", help="serve: arrival rates (req/s)")
-    ap.add_argument("--duration", type=float, default=3.0, help="serve: seconds of arrivals per rate")
+    ap.add_argument("--rates", default=SERVE_RATES, help="serve: arrival rates (req/s)")
+    ap.add_argument("--duration", type=float, default=20.0, help="serve: seconds of arrivals per rate")
+    ap.add_argument("--serve-duration", type=float, default=8.0,
+                    help="default workload: seconds of arrivals per rate of the serving sweep in its line "
+                         "(0 leaves the sweep out)")
     ap.add_argument("--budget-gb", type=float, default=4.0, help="serve: HBM admission budget")
     ap.add_argument("--instances", type=int, default=64)
     ap.add_argument("--vpls", type=int, default=0,

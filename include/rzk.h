@@ -640,6 +640,12 @@ rzk_status rzk_server_cancel(rzk_server *server, uint64_t ticket);
 /* Counters since creation; `launches` counts the kernels the server has launched. */
 rzk_status rzk_server_stats(rzk_server *server, int64_t *submitted, int64_t *rejected, int64_t *completed,
                             int64_t *launches, int64_t *held_bytes, int64_t *budget_bytes);
+/* Where each completed request's latency went, in completion order (the first `cap`, at
+ * most 2^20 kept): its kind, the time from submit to the launch of its group (waiting for a
+ * slot) and from that launch to completion (the group on its stream, behind the group
+ * before it).  *n receives the number recorded. */
+rzk_status rzk_server_timings(rzk_server *server, int32_t *h_kind, double *h_queue_ms, double *h_run_ms, int cap,
+                              int32_t *n);
 
 #ifdef __cplusplus
 }

@@ -2,23 +2,31 @@
 //
 // Callers submit gather or guided-render requests (rzk_server_submit) from any thread.  A
 // request is admitted only if the device memory it will hold while in flight (its receivers
-// and, for a gather, its per-chunk partial sums) fits the server's HBM budget next to the
-// requests already admitted; otherwise the call returns RZK_ERR_BUSY at once and the caller
-// decides whether to retry.  One worker thread owns a context and a stream and keeps at
-// most two launch groups on it (one running, one queued behind it, so the GPU never waits
-// for the host).  Whenever a slot frees it re-orders everything not yet launched - requests
-// waiting over 2 s first, then shortest estimated work first - and issues the next group:
-// consecutive gathers as ONE persistent batched launch of at most ~2e9 evaluations, or one
-// guided render (continuous batching: new requests compete for the very next slot).  A host
-// function after a group's last kernel marks its requests done.  With batching off the
-// worker issues one request at a time in arrival order with its own launches (the plain
-// per-request baseline).  Scratch comes from the stream-ordered allocator, so an iteration
-// neither blocks on an allocation nor synchronises the device.
+// and, for a gather, its per-chunk partial sums and spatially ordered VPL copy; for a guided
+// render, its per-path radiance and chain pool) fits the server's HBM budget next to the
+// requests already admitted, and the device's free memory (sampled by the worker) has room
+// for it; otherwise the call returns RZK_ERR_BUSY at once and the caller decides whether to
+// retry.
+//
+// One worker thread owns a context and two streams ("lanes"): gathers run on one, guided
+// renders on the other, so the two kinds of work overlap on the device - a guided render's
+// paths fill the SMs a finishing gather frees and the reverse.  Each lane keeps at most two
+// launch groups queued on its stream (one running, one behind it, so the GPU never waits for
+// the host).  Whenever a lane has room the worker issues its next group from the requests
+// not yet launched, in arrival order: on the gather lane every waiting gather, oldest first,
+// as ONE persistent batched launch of at most ~2e9 evaluations (a request larger than that
+// goes alone); on the guided lane the oldest guided render.  Continuous batching: a request
+// that arrives while others run joins the lane's very next group.  A host function after a
+// group's last kernel marks its requests done.  With batching off the worker issues one
+// request at a time in arrival order, with its own launches, on one stream (the plain
+// per-request baseline).  Scratch comes from the stream-ordered allocator, whose pool keeps
+// freed blocks, so an iteration neither blocks on an allocation nor synchronises the device.
 #include "rzk_internal.cuh"
 
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstdint>
 #include <deque>
 #include <mutex>
 #include <thread>
@@ -32,6 +40,7 @@ double now_ms() {
 }
 
 enum { kQueued = 0, kRunning = 1, kDone = 2, kCancelled = 3, kFailed = 4 };
+enum { kLaneGather = 0, kLaneGuided = 1, kLanes = 2 };
 
 struct Req {
     uint64_t id = 0;
@@ -39,15 +48,16 @@ struct Req {
     size_t bytes = 0;
     int state = kQueued;
     rzk_status status = RZK_OK;
-    double t_submit = 0.0, t_done = 0.0;
+    double t_submit = 0.0, t_launch = 0.0, t_done = 0.0;
     rzk_receiver *d_recv = nullptr;
-    double cost = 0.0;        // estimated work, for ordering an iteration
-    struct rzk_server *srv = nullptr;
+    float *d_paths = nullptr;
+    double cost = 0.0;        // estimated work (evaluations, or paths x 32)
 };
 
-constexpr double kLaunchCost = 2e9;   // work of one batched launch (~0.1 s of gather)
-constexpr double kAgeMs = 2000.0;     // waiting longer than this overrides shortest-first
-constexpr int kMaxInFlight = 2;       // launch groups on the stream: one running, one queued
+constexpr double kLaunchCost = 2e9;     // work of one batched launch (~30 ms of gather)
+constexpr int kMaxInFlight = 2;         // launch groups per lane: one running, one queued
+constexpr int64_t kFreeReserve = 256ll << 20;   // device memory never handed to requests
+constexpr size_t kTimingCap = 1 << 20;  // completed requests whose timings are kept
 
 int default_chunks(int n_vpl) {   // rzk_gather's automatic chunk count
     const int max_chunks = std::max(1, (n_vpl + 127) / 128);
@@ -59,27 +69,31 @@ int default_chunks(int n_vpl) {   // rzk_gather's automatic chunk count
 struct rzk_server {
     int device = 0;
     rzk_context *ctx = nullptr;
-    cudaStream_t st = nullptr;
+    cudaStream_t st[kLanes] = {nullptr, nullptr};
     rzk_server_params prm{};
-    int64_t budget = 0, held = 0;
+    int64_t budget = 0, held = 0, free_bytes = 0;
     int64_t n_submitted = 0, n_rejected = 0, n_completed = 0, n_launches = 0;
     uint64_t next_id = 1;
     bool stop = false;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::deque<Req *> queue;     // submitted, not yet seen by the worker
-    std::vector<Req *> ready;    // seen by the worker, not yet launched
-    int in_flight = 0;           // launch groups issued and not finished
+    std::vector<Req *> ready;    // seen by the worker, not yet launched (arrival order)
+    int in_flight[kLanes] = {0, 0};   // launch groups issued and not finished, per lane
     std::unordered_map<uint64_t, Req *> reqs;
+    // per completed request: kind, queue wait (submit -> launch) and run (launch -> done), ms
+    std::vector<int32_t> t_kind;
+    std::vector<double> t_queue, t_run;
     std::thread worker;
 };
 
 namespace {
 
-// One launch group: the requests whose kernels were issued together; the host function
-// after the group's last kernel marks them done.
+// One launch group: the requests whose kernels were issued together on one lane; the host
+// function after the group's last kernel marks them done.
 struct Group {
     rzk_server *s = nullptr;
+    int lane = kLaneGather;
     std::vector<Req *> reqs;
     int64_t launches = 0;
 };
@@ -95,19 +109,24 @@ void CUDART_CB on_group_done(void *p) {
             q->state = q->status == RZK_OK ? kDone : kFailed;
             s->held -= (int64_t)q->bytes;
             s->n_completed++;
+            if (s->t_kind.size() < kTimingCap) {
+                s->t_kind.push_back(q->r.kind);
+                s->t_queue.push_back(q->t_launch - q->t_submit);
+                s->t_run.push_back(t - q->t_launch);
+            }
         }
         s->n_launches += g->launches;
-        s->in_flight--;
+        s->in_flight[g->lane]--;
     }
     s->cv_done.notify_all();
     s->cv_work.notify_all();
     delete g;
 }
 
-// Issues one group: every request's primary hits, then its gathers as one batched launch
-// (or, without batching, the request's own launches) or its guided render.
+// Issues one group on its lane's stream: every request's primary hits, then its gathers as
+// one batched launch (or, without batching, the request's own launches) or its guided render.
 void launch_group(rzk_server *s, Group *g) {
-    cudaStream_t st = s->st;
+    cudaStream_t st = s->st[g->lane];
     std::vector<Req *> live;
     for (Req *q : g->reqs) {
         const size_t n = (size_t)q->r.camera.width * q->r.camera.height;
@@ -124,8 +143,15 @@ void launch_group(rzk_server *s, Group *g) {
     for (Req *q : live) {
         const rzk_request &r = q->r;
         if (r.kind == RZK_REQ_GUIDED) {
+            const size_t n = (size_t)r.camera.width * r.camera.height;
+            // the per-path radiance in the request's own buffer (no context scratch to grow)
+            if (cudaMallocAsync((void **)&q->d_paths, sizeof(float) * 3 * n * (size_t)r.spp, st) != cudaSuccess) {
+                q->d_paths = nullptr;
+                q->status = RZK_ERR_NOMEM;
+                continue;
+            }
             rzk_guided_params gp{r.spp, r.max_bounce, r.rr_depth, r.rr_prob, 1, r.seed, r.sampler, 0};
-            q->status = rzk_guided_render(s->ctx, r.scene, r.lightslice, &r.camera, &gp, r.d_rgb, nullptr, st);
+            q->status = rzk_guided_render(s->ctx, r.scene, r.lightslice, &r.camera, &gp, r.d_rgb, q->d_paths, st);
             g->launches += r.sampler == RZK_GUIDE_METROPOLIS ? 3 : 2;   // (chains +) path kernel + per-pixel mean
         } else if (!s->prm.batching) {
             q->status = rzk_gather_cfg(s->ctx, r.scene, q->d_recv, r.camera.width * r.camera.height, r.camera.width,
@@ -162,8 +188,12 @@ void launch_group(rzk_server *s, Group *g) {
         if (plan) rzk::batch_plan_destroy(plan);
         for (Req *q : gathers) q->status = r;
     }
-    for (Req *q : g->reqs)
+    for (Req *q : g->reqs) {
         if (q->d_recv) cudaFreeAsync(q->d_recv, st);
+        if (q->d_paths) cudaFreeAsync(q->d_paths, st);
+        q->d_recv = nullptr;
+        q->d_paths = nullptr;
+    }
     if (cudaLaunchHostFunc(st, on_group_done, g) != cudaSuccess) {
         // the stream cannot run host functions: finish the group here
         cudaStreamSynchronize(st);
@@ -173,41 +203,48 @@ void launch_group(rzk_server *s, Group *g) {
     }
 }
 
-// Picks the next group from the ready list (called with the lock held).  Batching:
-// requests waiting longer than kAgeMs first in arrival order, then shortest estimated work
-// first; consecutive gathers form one group while their total work stays within
-// kLaunchCost; a guided render is a group of its own.  Without batching: arrival order,
-// one request per group.
+int lane_of(const rzk_server *s, const Req *q) {
+    if (!s->prm.batching) return kLaneGather;   // the plain loop: one stream
+    return q->r.kind == RZK_REQ_GUIDED ? kLaneGuided : kLaneGather;
+}
+
+// Picks the next group for a lane with room (called with the lock held), or nullptr.
+// Batching: the gather lane takes every waiting gather in arrival order while their total
+// work stays within kLaunchCost (at least one); the guided lane takes the oldest guided
+// render.  Without batching: the oldest request, alone.
 Group *next_group(rzk_server *s) {
     std::vector<Req *> &rd = s->ready;
     if (rd.empty()) return nullptr;
-    Group *g = new Group();
-    g->s = s;
     if (!s->prm.batching) {
+        if (s->in_flight[kLaneGather] >= kMaxInFlight) return nullptr;
+        Group *g = new Group();
+        g->s = s;
         g->reqs.push_back(rd.front());
         rd.erase(rd.begin());
         return g;
     }
-    const double now = now_ms();
-    std::stable_sort(rd.begin(), rd.end(), [now](const Req *a, const Req *b) {
-        const bool aa = now - a->t_submit > kAgeMs, ab = now - b->t_submit > kAgeMs;
-        if (aa != ab) return aa;
-        if (aa) return a->id < b->id;
-        return a->cost < b->cost;
-    });
-    const int max_batch = s->prm.max_batch > 0 ? s->prm.max_batch : 256;
-    size_t take = 1;
-    if (rd.front()->r.kind == RZK_REQ_GATHER) {
-        double cost = rd.front()->cost;
-        while (take < rd.size() && (int)take < max_batch && rd[take]->r.kind == RZK_REQ_GATHER &&
-               cost + rd[take]->cost <= kLaunchCost) {
-            cost += rd[take]->cost;
-            ++take;
+    for (int lane : {kLaneGather, kLaneGuided}) {
+        if (s->in_flight[lane] >= kMaxInFlight) continue;
+        const int max_batch = lane == kLaneGuided ? 1 : (s->prm.max_batch > 0 ? s->prm.max_batch : 256);
+        std::vector<Req *> take;
+        double cost = 0.0;
+        for (Req *q : rd) {
+            if (lane_of(s, q) != lane) continue;
+            if (!take.empty() && ((int)take.size() >= max_batch || cost + q->cost > kLaunchCost)) break;
+            take.push_back(q);
+            cost += q->cost;
         }
+        if (take.empty()) continue;
+        Group *g = new Group();
+        g->s = s;
+        g->lane = lane;
+        g->reqs = take;
+        rd.erase(std::remove_if(rd.begin(), rd.end(),
+                                [&](Req *q) { return std::find(take.begin(), take.end(), q) != take.end(); }),
+                 rd.end());
+        return g;
     }
-    g->reqs.assign(rd.begin(), rd.begin() + take);
-    rd.erase(rd.begin(), rd.begin() + take);
-    return g;
+    return nullptr;
 }
 
 void worker_main(rzk_server *s) {
@@ -215,23 +252,36 @@ void worker_main(rzk_server *s) {
     while (true) {
         Group *g = nullptr;
         {
+            size_t fr = 0, tot = 0;
+            if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) {
+                std::lock_guard<std::mutex> lk(s->mu);
+                s->free_bytes = (int64_t)fr;
+            }
             std::unique_lock<std::mutex> lk(s->mu);
             s->cv_work.wait(lk, [&] {
-                const bool work = !s->queue.empty() || !s->ready.empty();
-                return (s->stop && !work) || (work && s->in_flight < kMaxInFlight);
+                while (!s->queue.empty()) {
+                    s->ready.push_back(s->queue.front());
+                    s->queue.pop_front();
+                }
+                if (s->ready.empty()) return s->stop;
+                for (Req *q : s->ready)
+                    if (s->in_flight[lane_of(s, q)] < kMaxInFlight) return true;
+                return false;
             });
-            while (!s->queue.empty()) {
-                s->ready.push_back(s->queue.front());
-                s->queue.pop_front();
-            }
             if (s->ready.empty()) break;   // stopping and drained
             g = next_group(s);
-            for (Req *q : g->reqs) q->state = kRunning;
-            s->in_flight++;
+            if (!g) continue;
+            const double t = now_ms();
+            for (Req *q : g->reqs) {
+                q->state = kRunning;
+                q->t_launch = t;
+            }
+            s->in_flight[g->lane]++;
         }
         launch_group(s, g);
     }
-    cudaStreamSynchronize(s->st);
+    for (cudaStream_t st : s->st)
+        if (st) cudaStreamSynchronize(st);
 }
 
 }  // namespace
@@ -250,17 +300,26 @@ rzk_status rzk_server_create(int device, const rzk_server_params *params, rzk_se
         delete s;
         return r;
     }
-    if (cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) != cudaSuccess) {
-        rzk_context_destroy(s->ctx);
-        delete s;
-        return RZK_ERR_CUDA;
+    for (cudaStream_t &st : s->st)
+        if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+            for (cudaStream_t x : s->st)
+                if (x) cudaStreamDestroy(x);
+            rzk_context_destroy(s->ctx);
+            delete s;
+            return RZK_ERR_CUDA;
+        }
+    // the stream-ordered pool keeps freed blocks for the next requests instead of returning
+    // them to the driver at every synchronisation
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
     }
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    s->free_bytes = (int64_t)fr;
     s->budget = params->hbm_budget_bytes;
-    if (s->budget == 0) {
-        size_t fr = 0, tot = 0;
-        cudaMemGetInfo(&fr, &tot);
-        s->budget = (int64_t)(0.9 * (double)fr);
-    }
+    if (s->budget == 0) s->budget = (int64_t)(0.9 * (double)fr);
     s->worker = std::thread(worker_main, s);
     *out = s;
     return RZK_OK;
@@ -274,9 +333,11 @@ rzk_status rzk_server_destroy(rzk_server *s) {
     }
     s->cv_work.notify_all();
     if (s->worker.joinable()) s->worker.join();
-    cudaStreamSynchronize(s->st);
+    for (cudaStream_t st : s->st) {
+        cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
+    }
     for (auto &kv : s->reqs) delete kv.second;
-    cudaStreamDestroy(s->st);
     rzk_context_destroy(s->ctx);
     delete s;
     return RZK_OK;
@@ -300,13 +361,26 @@ rzk_status rzk_server_submit(rzk_server *s, const rzk_request *req, uint64_t *ti
             (r.rr_depth > 0 && !(r.rr_prob > 0.0f && r.rr_prob <= 1.0f)) ||
             (r.sampler != RZK_GUIDE_JENSEN && r.sampler != RZK_GUIDE_METROPOLIS))
             return RZK_ERR_INVALID;
+        if (n * (int64_t)r.spp > (1LL << 31)) return RZK_ERR_CAPACITY;
+        // the per-path radiance, and the Metropolis chains' pool (4,096 states per slice)
+        bytes += sizeof(float) * 3 * (size_t)n * (size_t)r.spp;
+        if (r.sampler == RZK_GUIDE_METROPOLIS) {
+            int32_t ns = 0;
+            if (rzk_lightslice_info(r.lightslice, nullptr, &ns, nullptr, nullptr, nullptr, nullptr) == RZK_OK)
+                bytes += 16 * 4096 * (size_t)std::max(ns, 0);
+        }
     } else {
         return RZK_ERR_INVALID;
     }
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->stop) return RZK_ERR_INVALID;
     s->n_submitted++;
-    if (s->held + (int64_t)bytes > s->budget) {
+    // the budget, and the device's free memory as the worker last sampled it, minus what the
+    // admitted but not yet launched requests will take from it
+    int64_t pending = 0;
+    for (Req *q : s->queue) pending += (int64_t)q->bytes;
+    for (Req *q : s->ready) pending += (int64_t)q->bytes;
+    if (s->held + (int64_t)bytes > s->budget || (int64_t)bytes + pending > s->free_bytes - kFreeReserve) {
         s->n_rejected++;
         return RZK_ERR_BUSY;
     }
@@ -314,7 +388,6 @@ rzk_status rzk_server_submit(rzk_server *s, const rzk_request *req, uint64_t *ti
     q->id = s->next_id++;
     q->r = r;
     q->bytes = bytes;
-    q->srv = s;
     q->t_submit = now_ms();
     q->cost = r.kind == RZK_REQ_GATHER ? (double)n * (double)std::max(r.n_vpl, 1) : (double)n * r.spp * 32.0;
     s->held += (int64_t)bytes;
@@ -390,6 +463,18 @@ rzk_status rzk_server_stats(rzk_server *s, int64_t *submitted, int64_t *rejected
     if (launches) *launches = s->n_launches;
     if (held_bytes) *held_bytes = s->held;
     if (budget_bytes) *budget_bytes = s->budget;
+    return RZK_OK;
+}
+
+rzk_status rzk_server_timings(rzk_server *s, int32_t *h_kind, double *h_queue_ms, double *h_run_ms, int cap,
+                              int32_t *n) {
+    if (!s || !n || cap < 0 || (cap > 0 && (!h_kind || !h_queue_ms || !h_run_ms))) return RZK_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(s->mu);
+    const int k = (int)std::min<size_t>((size_t)cap, s->t_kind.size());
+    std::copy(s->t_kind.begin(), s->t_kind.begin() + k, h_kind);
+    std::copy(s->t_queue.begin(), s->t_queue.begin() + k, h_queue_ms);
+    std::copy(s->t_run.begin(), s->t_run.begin() + k, h_run_ms);
+    *n = (int32_t)s->t_kind.size();
     return RZK_OK;
 }
 

@@ -116,6 +116,7 @@ SIGNATURES = [
     ("rzk_server_wait", I32, [P, ctypes.c_uint64, I32, P]),
     ("rzk_server_cancel", I32, [P, ctypes.c_uint64]),
     ("rzk_server_stats", I32, [P, P, P, P, P, P, P]),
+    ("rzk_server_timings", I32, [P, P, P, P, I32, P]),
 ]
 
 _LIB = None
@@ -967,6 +968,18 @@ class Server:
         check(self.lib.rzk_server_stats(self.h, *[ctypes.byref(x) for x in v]), "rzk_server_stats")
         return dict(zip(["submitted", "rejected", "completed", "launches", "held_bytes", "budget_bytes"],
                         [x.value for x in v]))
+
+    def timings(self):
+        """Per completed request (completion order): kind, queue wait and run time in ms
+        (rzk_server_timings)."""
+        n = I32()
+        check(self.lib.rzk_server_timings(self.h, None, None, None, 0, ctypes.byref(n)), "rzk_server_timings")
+        k = n.value
+        kind = np.zeros(k, np.int32)
+        qm, rm = np.zeros(k, np.float64), np.zeros(k, np.float64)
+        check(self.lib.rzk_server_timings(self.h, kind.ctypes.data, qm.ctypes.data, rm.ctypes.data, k,
+                                          ctypes.byref(n)), "rzk_server_timings")
+        return kind, qm, rm
 
     def close(self):
         if getattr(self, "h", None):

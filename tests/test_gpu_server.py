@@ -81,6 +81,9 @@ def test_server_results_equal_direct_calls(ctx, world, batching):
         assert st == rzk.OK and lat >= 0.0
     stats = srv.stats()
     assert stats["completed"] == len(reqs) and stats["held_bytes"] == 0
+    kind, queue_ms, run_ms = srv.timings()
+    assert len(kind) == len(reqs) and sorted(kind) == sorted(int(r["req"].kind) for r in reqs)
+    assert np.all(queue_ms >= 0) and np.all(run_ms >= 0)
     srv.close()
     for r in reqs:
         got = r["out"].cpu().numpy()
