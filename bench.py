@@ -557,7 +557,7 @@ def run_batch(args):
 
     jobs = rzk.make_jobs(i.job() for i in insts)
     t0 = time.perf_counter()
-    variant, chunk_len, probe_ms = rzk.autotune_batch(ctx, jobs, max_probe_jobs=8)
+    variant, chunk_len, probe_ms, probes = rzk.autotune_batch(ctx, jobs, max_probe_jobs=8, table=True)
     tune_s = time.perf_counter() - t0
     batch = rzk.GatherBatch(ctx, jobs, variant=variant, chunk_len=chunk_len)
     batch.run()
@@ -595,7 +595,12 @@ def run_batch(args):
                    "l2": "flushed between timed steps (256 MiB write)"},
         "plain_launches": {"value": evals / mp, "ms_per_step": 1e3 * mp, "launches_per_step": 3 * len(insts)},
         "speedup_vs_plain": mp / mg,
-        "autotune": {"variant": variant, "chunk_len": chunk_len, "probe_ms": probe_ms, "tune_s": tune_s},
+        "autotune": {"variant": variant, "shape": rzk.batch_variant_info(variant), "chunk_len": chunk_len,
+                     "probe_ms": probe_ms, "tune_s": tune_s,
+                     "search": [{"variant": v, "shape": rzk.batch_variant_info(v),
+                                 "ms_by_chunk_len": dict(zip(["default", "512", "1024", "2048"],
+                                                             [float(x) for x in probes[v]]))}
+                                for v in range(probes.shape[0])]},
         "max_rel_diff_vs_plain": rel, "gpu_launches": graph_launches * args.steps,
         "gpu_launches_note": f"{graph_launches} kernel nodes in the replayed graph per step",
         "clocks": clk.summary(),

@@ -357,8 +357,14 @@ typedef struct {
 
 typedef struct rzk_batch rzk_batch;
 
-/* Number of compiled batch tile configurations (warps per CTA, VPLs per tile, CTAs/SM). */
+/* Number of compiled batch tile configurations (warps per CTA, VPLs per tile, CTAs/SM,
+ * warp tile shape). */
 int rzk_batch_variants(void);
+/* A batch variant's tile shape: warps per CTA (each warp one 32-receiver packet, one lane
+ * per shadow ray), VPLs per shared-memory tile, resident CTAs per SM it is compiled for, and
+ * the warp tile's width in pixels (8: 8 x 4 receivers; 4: 4 x 8; 16: 16 x 2; 32: 32 x 1). */
+rzk_status rzk_batch_variant_info(int variant, int32_t *warps, int32_t *vpl_tile, int32_t *ctas_per_sm,
+                                  int32_t *tile_width);
 
 /* Describes a batch of independent gathers (the integrator's per-frame gather of
  * vpl.cc:496-520 for many scenes or requests at once): uploads a device job table and
@@ -374,12 +380,13 @@ rzk_status rzk_batch_create(rzk_context *ctx, const rzk_gather_job *jobs, int n_
  * Each job's image equals rzk_gather_cfg's for the same chunk length, bit for bit. */
 rzk_status rzk_batch_run(rzk_batch *batch, void *stream);
 rzk_status rzk_batch_destroy(rzk_batch *batch);
-/* Autotuner: times every batch variant x chunk length in {default (0), 512, 1024, 2048}
- * (best of two runs each) on up to max_probe_jobs evenly spaced jobs (0 = all) and returns
- * the fastest.  Synchronises `stream`. */
+/* Autotuner: times every batch variant (tile shape) x chunk length in {default (0), 512,
+ * 1024, 2048} (best of two runs each) on up to max_probe_jobs evenly spaced jobs (0 = all)
+ * and returns the fastest; h_probe_ms (NULL or rzk_batch_variants() x 4 floats, variant-major)
+ * receives every probe's time.  Synchronises `stream`. */
 rzk_status rzk_batch_autotune(rzk_context *ctx, const rzk_gather_job *jobs, int n_jobs,
                               int max_probe_jobs, int *best_variant, int *best_chunk_len,
-                              float *best_ms, void *stream);
+                              float *best_ms, float *h_probe_ms, void *stream);
 
 /* Clustering ------------------------------------------------------------------------- */
 

@@ -55,7 +55,7 @@ __device__ __forceinline__ int find_job(const JobTable &t, long long item, bool 
     return lo;
 }
 
-template <int WARPS, int TILE, int MINB>
+template <int WARPS, int TILE, int MINB, int TW = 8>
 __global__ void __launch_bounds__(WARPS * 32, MINB) batch_gather_kernel(const __grid_constant__ JobTable t,
                                                                         int *work) {
     __shared__ __align__(128) rzk_vpl tiles[WARPS][2][TILE];
@@ -74,8 +74,8 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) batch_gather_kernel(const __
         const int local = item - (int)jb.item_begin;
         const int wt = local / jb.n_chunks;   // tile-major, as gather_persistent_kernel
         const int chunk = local - wt * jb.n_chunks;
-        if (!gather_item<TILE>(jb.s, jb.recv, jb.n_recv, jb.img_w, jb.vpls, jb.n_vpl, chunk, wt, jb.chunk_len,
-                               jb.mode, jb.tau, jb.partial, ws, lane))
+        if (!gather_item<TILE, TW>(jb.s, jb.recv, jb.n_recv, jb.img_w, jb.vpls, jb.n_vpl, chunk, wt,
+                                   jb.chunk_len, jb.mode, jb.tau, jb.partial, ws, lane))
             break;
     }
 }
@@ -92,17 +92,24 @@ __global__ void batch_reduce_kernel(const __grid_constant__ JobTable t) {
     jb.out[k] = acc * jb.scale;
 }
 
+// The tile shapes the autotuner searches: warps per CTA (x 32 receivers, one lane per
+// shadow ray: the warp is the packet), VPLs per shared-memory tile, resident CTAs per SM
+// (the register cap), and the warp tile's width in pixels (8 x 4, 4 x 8, 16 x 2, 32 x 1).
+// The traversal stack stays at the reference's 64 entries (256 bytes of shared memory per
+// warp, which never limits residency).
 struct BatchVariant {
-    int warps, tile, minb;
+    int warps, tile, minb, tw;
 };
-const BatchVariant kBatchVariants[] = {{4, 32, 5}, {4, 32, 4}, {2, 32, 1}, {4, 16, 5}};
+const BatchVariant kBatchVariants[] = {{4, 32, 5, 8}, {4, 32, 4, 8}, {2, 32, 1, 8}, {4, 16, 5, 8},
+                                       {4, 32, 5, 4}, {4, 32, 5, 16}, {4, 32, 5, 32}};
 
-template <int WARPS, int TILE, int MINB>
+template <int WARPS, int TILE, int MINB, int TW = 8>
 int batch_grid() {
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_gather_kernel<WARPS, TILE, MINB>, WARPS * 32, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_gather_kernel<WARPS, TILE, MINB, TW>, WARPS * 32,
+                                                  0);
     return std::max(1, sms * std::max(1, per_sm));
 }
 
@@ -111,6 +118,9 @@ int grid_for(int variant) {
         case 0: return batch_grid<4, 32, 5>();
         case 1: return batch_grid<4, 32, 4>();
         case 2: return batch_grid<2, 32, 1>();
+        case 4: return batch_grid<4, 32, 5, 4>();
+        case 5: return batch_grid<4, 32, 5, 16>();
+        case 6: return batch_grid<4, 32, 5, 32>();
         default: return batch_grid<4, 16, 5>();
     }
 }
@@ -136,7 +146,13 @@ struct BatchPlan {
 
 static size_t up256(size_t b) { return (b + 255) & ~(size_t)255; }
 
-rzk_status batch_plan_create(const rzk_gather_job *jobs, int n_jobs, int chunk_len, BatchPlan **out) {
+int batch_variant_tile_width(int variant) {
+    return variant >= 0 && variant < (int)(sizeof(kBatchVariants) / sizeof(kBatchVariants[0]))
+               ? kBatchVariants[variant].tw : 8;
+}
+
+rzk_status batch_plan_create(const rzk_gather_job *jobs, int n_jobs, int chunk_len, int tile_width,
+                             BatchPlan **out) {
     if (!jobs || n_jobs <= 0 || !out || chunk_len < 0 || (chunk_len % 128) != 0) return RZK_ERR_INVALID;
     *out = nullptr;
     std::vector<BatchJob> h(n_jobs);
@@ -158,13 +174,10 @@ rzk_status batch_plan_create(const rzk_gather_job *jobs, int n_jobs, int chunk_l
         b.mode = g.clamp_mode;
         b.tau = g.tau;
         b.scale = g.scale;
-        long long wtiles;
-        if (b.img_w > 0) {
-            long long img_h = ((long long)b.n_recv + b.img_w - 1) / b.img_w;
-            wtiles = (long long)((b.img_w + 7) / 8) * ((img_h + 3) / 4);
-        } else {
-            wtiles = ((long long)b.n_recv + 31) / 32;
-        }
+        const long long wtiles = tile_width == 4    ? warp_tiles<4>(b.n_recv, b.img_w)
+                                 : tile_width == 16 ? warp_tiles<16>(b.n_recv, b.img_w)
+                                 : tile_width == 32 ? warp_tiles<32>(b.n_recv, b.img_w)
+                                                    : warp_tiles<8>(b.n_recv, b.img_w);
         b.n_wtiles = (int)wtiles;
         int cl = chunk_len;
         if (cl == 0) {   // the default of rzk_gather: at most 32 chunks of a multiple of 128 VPLs
@@ -253,6 +266,9 @@ rzk_status batch_plan_launch(BatchPlan *p, float *partial, void *order, int *wor
             case 0: batch_gather_kernel<4, 32, 5><<<grid, 128, 0, st>>>(t, w); break;
             case 1: batch_gather_kernel<4, 32, 4><<<grid, 128, 0, st>>>(t, w); break;
             case 2: batch_gather_kernel<2, 32, 1><<<grid, 64, 0, st>>>(t, w); break;
+            case 4: batch_gather_kernel<4, 32, 5, 4><<<grid, 128, 0, st>>>(t, w); break;
+            case 5: batch_gather_kernel<4, 32, 5, 16><<<grid, 128, 0, st>>>(t, w); break;
+            case 6: batch_gather_kernel<4, 32, 5, 32><<<grid, 128, 0, st>>>(t, w); break;
             default: batch_gather_kernel<4, 16, 5><<<grid, 128, 0, st>>>(t, w); break;
         }
         RZK_CUDA_TRY(cudaGetLastError());
@@ -295,7 +311,7 @@ rzk_status rzk_batch_create(rzk_context *ctx, const rzk_gather_job *jobs, int n_
     if (chunk_len < 0 || (chunk_len % 128) != 0) return RZK_ERR_INVALID;
     *out = nullptr;
     BatchPlan *plan = nullptr;
-    rzk_status r = batch_plan_create(jobs, n_jobs, chunk_len, &plan);
+    rzk_status r = batch_plan_create(jobs, n_jobs, chunk_len, batch_variant_tile_width(variant), &plan);
     if (r != RZK_OK) return r;
     rzk_batch *bt = new rzk_batch();
     bt->ctx = ctx;
@@ -323,8 +339,20 @@ rzk_status rzk_batch_run(rzk_batch *b, void *stream) {
                              (cudaStream_t)stream);
 }
 
+rzk_status rzk_batch_variant_info(int variant, int32_t *warps, int32_t *vpl_tile, int32_t *ctas_per_sm,
+                                  int32_t *tile_width) {
+    if (variant < 0 || variant >= rzk_batch_variants()) return RZK_ERR_INVALID;
+    const BatchVariant &v = kBatchVariants[variant];
+    if (warps) *warps = v.warps;
+    if (vpl_tile) *vpl_tile = v.tile;
+    if (ctas_per_sm) *ctas_per_sm = v.minb;
+    if (tile_width) *tile_width = v.tw;
+    return RZK_OK;
+}
+
 rzk_status rzk_batch_autotune(rzk_context *ctx, const rzk_gather_job *jobs, int n_jobs, int max_probe_jobs,
-                              int *best_variant, int *best_chunk_len, float *best_ms, void *stream) {
+                              int *best_variant, int *best_chunk_len, float *best_ms, float *h_probe_ms,
+                              void *stream) {
     if (!ctx || !jobs || n_jobs <= 0 || !best_variant || !best_chunk_len) return RZK_ERR_INVALID;
     // probe on an evenly spaced subset of the jobs (all of them if max_probe_jobs <= 0)
     std::vector<rzk_gather_job> probe;
@@ -340,7 +368,8 @@ rzk_status rzk_batch_autotune(rzk_context *ctx, const rzk_gather_job *jobs, int 
     *best_chunk_len = 0;
     rzk_status res = RZK_OK;
     for (int v = 0; v < rzk_batch_variants() && res == RZK_OK; ++v) {
-        for (int c : chunks) {
+        for (int ci = 0; ci < 4; ++ci) {
+            const int c = chunks[ci];
             rzk_batch *bt = nullptr;
             res = rzk_batch_create(ctx, probe.data(), (int)probe.size(), v, c, &bt);
             if (res != RZK_OK) break;
@@ -356,6 +385,7 @@ rzk_status rzk_batch_autotune(rzk_context *ctx, const rzk_gather_job *jobs, int 
                 ms = std::min(ms, t);
             }
             rzk_batch_destroy(bt);
+            if (h_probe_ms) h_probe_ms[v * 4 + ci] = ms;
             if (res == RZK_OK && ms < best) {
                 best = ms;
                 *best_variant = v;

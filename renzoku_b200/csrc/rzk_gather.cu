@@ -367,7 +367,7 @@ __global__ void __launch_bounds__(WARPS * 32) gather_packet_kernel(DevScene s, c
 // order; chunk partial sums are added in chunk order by reduce_chunks_kernel.
 // ---------------------------------------------------------------------------------
 
-template <int WARPS, int TILE, int MINB>
+template <int WARPS, int TILE, int MINB, int TW = 8>
 __global__ void __launch_bounds__(WARPS * 32, MINB) gather_persistent_kernel(
     DevScene s, const rzk_receiver *recv, int n_recv, int img_w, const rzk_vpl *vpls, int n_vpl,
     int chunk_len, int n_chunks, int n_wtiles, int *work, int mode, float tau, float *partial) {
@@ -388,8 +388,8 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) gather_persistent_kernel(
         // band of ray origins) against every chunk
         const int wt = item / n_chunks;
         const int chunk = item - wt * n_chunks;
-        if (!gather_item<TILE>(s, recv, n_recv, img_w, vpls, n_vpl, chunk, wt, chunk_len, mode, tau, partial,
-                               ws, lane))
+        if (!gather_item<TILE, TW>(s, recv, n_recv, img_w, vpls, n_vpl, chunk, wt, chunk_len, mode, tau, partial,
+                                   ws, lane))
             break;
     }
 }
@@ -665,27 +665,29 @@ static rzk_status order_gather_vpls(rzk_context *ctx, const float *box, const rz
 }
 
 // Tile configurations compiled in; the autotuner picks one per workload.
-//   kind 3: persistent warp-packet kernel (the production path)      variants 0-3
+//   kind 3: persistent warp-packet kernel (the production path)      variants 0-3, 8-10
 //           (0 and 3 cap registers for 5 and 6 resident 4-warp CTAs per SM; 0 is the
-//           default, fastest on the scaled scene)
+//           default, fastest on the scaled scene; 8-10 are variant 0 with warp tiles of
+//           4 x 8, 16 x 2 and 32 x 1 pixels instead of 8 x 4)
 //   kind 1: warp-packet kernel, one CTA per receiver block            variants 4-5
 //   kind 2: warp-packet kernel on the 4-wide tree                     variant 6
 //   kind 0: per-thread block-lockstep kernel (first implementation)   variant 7
 struct GatherVariant {
-    int kind, warps_or_block, tile;
+    int kind, warps_or_block, tile, tw;
 };
 static const GatherVariant kVariants[] = {
-    {3, 4, 32}, {3, 2, 32}, {3, 4, 32}, {3, 4, 32}, {1, 4, 32}, {1, 2, 32}, {2, 4, 32}, {0, 128, 64}};
+    {3, 4, 32, 8}, {3, 2, 32, 8}, {3, 4, 32, 8}, {3, 4, 32, 8}, {1, 4, 32, 8}, {1, 2, 32, 8}, {2, 4, 32, 8},
+    {0, 128, 64, 8}, {3, 4, 32, 4}, {3, 4, 32, 16}, {3, 4, 32, 32}};
 
 int gather_variant_count() { return (int)(sizeof(kVariants) / sizeof(kVariants[0])); }
 
-template <int WARPS, int TILE, int MINB>
+template <int WARPS, int TILE, int MINB, int TW = 8>
 static int persistent_grid(rzk_context *ctx, int variant) {
     if (ctx->persistent_grid[variant] == 0) {
         int dev = 0, sms = 0, per_sm = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gather_persistent_kernel<WARPS, TILE, MINB>,
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gather_persistent_kernel<WARPS, TILE, MINB, TW>,
                                                       WARPS * 32, 0);
         ctx->persistent_grid[variant] = std::max(1, sms * std::max(1, per_sm));
     }
@@ -727,13 +729,10 @@ rzk_status launch_gather(rzk_context *ctx, const DevScene &s, const float *box, 
     if (variant < 0 || variant >= gather_variant_count()) variant = 0;
     const GatherVariant gv = kVariants[variant];
     if (gv.kind == 0) img_w = 0;
-    long long wtiles;
-    if (img_w > 0) {
-        long long img_h = ((long long)n_recv + img_w - 1) / img_w;
-        wtiles = (long long)((img_w + 7) / 8) * ((img_h + 3) / 4);
-    } else {
-        wtiles = ((long long)n_recv + 31) / 32;
-    }
+    const long long wtiles = gv.tw == 4    ? warp_tiles<4>(n_recv, img_w)
+                             : gv.tw == 16 ? warp_tiles<16>(n_recv, img_w)
+                             : gv.tw == 32 ? warp_tiles<32>(n_recv, img_w)
+                                           : warp_tiles<8>(n_recv, img_w);
     int chunk_len = 0;
     resolve_chunks(n_vpl, n_chunks, chunk_len);
     size_t need = sizeof(float) * 3 * (size_t)n_recv * n_chunks;
@@ -754,6 +753,9 @@ rzk_status launch_gather(rzk_context *ctx, const DevScene &s, const float *box, 
             case 2: gather_persistent_kernel<4, 32, 1><<<persistent_grid<4, 32, 1>(ctx, 2), 128, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part); break;
             case 1: gather_persistent_kernel<2, 32, 1><<<persistent_grid<2, 32, 1>(ctx, 1), 64, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part); break;
             case 0: gather_persistent_kernel<4, 32, 5><<<persistent_grid<4, 32, 5>(ctx, 0), 128, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part); break;
+            case 8: gather_persistent_kernel<4, 32, 5, 4><<<persistent_grid<4, 32, 5, 4>(ctx, 8), 128, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part); break;
+            case 9: gather_persistent_kernel<4, 32, 5, 16><<<persistent_grid<4, 32, 5, 16>(ctx, 9), 128, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part); break;
+            case 10: gather_persistent_kernel<4, 32, 5, 32><<<persistent_grid<4, 32, 5, 32>(ctx, 10), 128, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part); break;
             default: gather_persistent_kernel<4, 32, 6><<<persistent_grid<4, 32, 6>(ctx, 3), 128, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part); break;
         }
     } else {

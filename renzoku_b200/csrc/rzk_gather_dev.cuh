@@ -90,16 +90,20 @@ __device__ __forceinline__ bool finite3(Rgb c) {
     return isfinite(c.r) && isfinite(c.g) && isfinite(c.b);
 }
 
-// Receiver index of a lane: an 8 x 4 tile of a row-major image of width img_w, or 32
+// Receiver index of a lane: a TW x (32 / TW) pixel tile of a row-major image of width
+// img_w (8 x 4 by default; the autotuner also tries 4 x 8, 16 x 2 and 32 x 1), or 32
 // consecutive receivers when img_w == 0.  -1 outside the receiver range.
+template <int TW = 8>
 __device__ __forceinline__ int lane_receiver(int gwarp, int lane, int n_recv, int img_w) {
+    static_assert(TW == 4 || TW == 8 || TW == 16 || TW == 32, "warp tile width");
+    constexpr int TH = 32 / TW;
     if (img_w <= 0) {
         int ri = gwarp * 32 + lane;
         return ri < n_recv ? ri : -1;
     }
-    int tiles_x = (img_w + 7) >> 3;
-    int x = (gwarp % tiles_x) * 8 + (lane & 7);
-    int y = (gwarp / tiles_x) * 4 + (lane >> 3);
+    int tiles_x = (img_w + TW - 1) / TW;
+    int x = (gwarp % tiles_x) * TW + (lane % TW);
+    int y = (gwarp / tiles_x) * TH + (lane / TW);
     if (x >= img_w) return -1;
     long long ri = (long long)y * img_w + x;
     return ri < n_recv ? (int)ri : -1;
@@ -292,14 +296,24 @@ struct WarpStage {
     }
 };
 
+// Warp tiles of an image (TW x (32 / TW) pixels each), or of 32 consecutive receivers
+// without an image width.
+template <int TW = 8>
+__host__ __device__ __forceinline__ long long warp_tiles(long long n_recv, int img_w) {
+    if (img_w <= 0) return (n_recv + 31) / 32;
+    const long long img_h = (n_recv + img_w - 1) / img_w;
+    return (long long)((img_w + TW - 1) / TW) * ((img_h + 32 / TW - 1) / (32 / TW));
+}
+
 // One work item of the persistent gather: the 32 receivers of warp tile `wt` against VPL
 // chunk `chunk`; writes that chunk's partial sums.  Returns false if a bounded wait gave
-// up (reported in the error word).
-template <int TILE>
+// up (reported in the error word).  The tile shape changes which receivers share a packet,
+// never a receiver's sum.
+template <int TILE, int TW = 8>
 __device__ __forceinline__ bool gather_item(const DevScene &s, const rzk_receiver *recv, int n_recv, int img_w,
                                             const rzk_vpl *vpls, int n_vpl, int chunk, int wt, int chunk_len,
                                             int mode, float tau, float *partial, WarpStage<TILE> &ws, int lane) {
-    const int ri = lane_receiver(wt, lane, n_recv, img_w);
+    const int ri = lane_receiver<TW>(wt, lane, n_recv, img_w);
     const int j0 = chunk * chunk_len;
     const int j1 = min(n_vpl, j0 + chunk_len);
     const int n_tiles = (j1 - j0 + TILE - 1) / TILE;

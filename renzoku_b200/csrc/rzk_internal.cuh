@@ -175,7 +175,9 @@ rzk_status ensure_scratch(rzk_context *ctx, size_t bytes);
 // buffer of batch_plan_partial_floats floats, an ordering buffer of batch_plan_order_bytes
 // bytes (16-byte aligned; null when that is 0) and batch_plan_tables work counters;
 // grid 0 = the variant's resident grid.
-rzk_status batch_plan_create(const rzk_gather_job *jobs, int n_jobs, int chunk_len, BatchPlan **out);
+rzk_status batch_plan_create(const rzk_gather_job *jobs, int n_jobs, int chunk_len, int tile_width,
+                             BatchPlan **out);
+int batch_variant_tile_width(int variant);   // warp tile width (pixels) of a batch variant
 void batch_plan_destroy(BatchPlan *p);
 size_t batch_plan_partial_floats(const BatchPlan *p);
 size_t batch_plan_order_bytes(const BatchPlan *p);

@@ -169,7 +169,7 @@ void launch_group(rzk_server *s, Group *g) {
                                      r.d_vpls, r.n_vpl, r.clamp_mode, r.tau, r.scale, r.d_rgb};
         }
         rzk::BatchPlan *plan = nullptr;
-        rzk_status r = rzk::batch_plan_create(jobs.data(), (int)jobs.size(), 0, &plan);
+        rzk_status r = rzk::batch_plan_create(jobs.data(), (int)jobs.size(), 0, 8, &plan);
         float *partial = nullptr;
         void *order = nullptr;
         int *work = nullptr;

@@ -91,7 +91,8 @@ SIGNATURES = [
     ("rzk_batch_create", I32, [P, P, I32, I32, I32, P]),
     ("rzk_batch_run", I32, [P, P]),
     ("rzk_batch_destroy", I32, [P]),
-    ("rzk_batch_autotune", I32, [P, P, I32, I32, P, P, P, P]),
+    ("rzk_batch_autotune", I32, [P, P, I32, I32, P, P, P, P, P]),
+    ("rzk_batch_variant_info", I32, [I32, P, P, P, P]),
     ("rzk_lightslice_params_default", I32, [P]),
     ("rzk_lightslice_create", I32, [P, P, P, I32, I32, P, I32, P, P, P]),
     ("rzk_lightslice_destroy", I32, [P]),
@@ -683,12 +684,26 @@ class GatherBatch:
             pass
 
 
-def autotune_batch(ctx: Context, jobs, max_probe_jobs=8, stream=None):
-    """Returns (variant, chunk_len, probe_ms) of the fastest batch configuration."""
+def batch_variant_info(variant: int) -> dict:
+    """A batch variant's tile shape (rzk_batch_variant_info)."""
+    lib = load()
+    w, t, m, tw = I32(), I32(), I32(), I32()
+    check(lib.rzk_batch_variant_info(variant, ctypes.byref(w), ctypes.byref(t), ctypes.byref(m), ctypes.byref(tw)),
+          "rzk_batch_variant_info")
+    return {"warps": w.value, "vpl_tile": t.value, "ctas_per_sm": m.value,
+            "warp_tile": f"{tw.value}x{32 // tw.value}"}
+
+
+def autotune_batch(ctx: Context, jobs, max_probe_jobs=8, stream=None, table: bool = False):
+    """Returns (variant, chunk_len, probe_ms) of the fastest batch configuration, and with
+    table=True also every probe's time [variants][4 chunk lengths: default, 512, 1024, 2048]."""
     lib = load()
     v, c, ms = I32(), I32(), ctypes.c_float()
+    probes = np.zeros((lib.rzk_batch_variants(), 4), np.float32)
     check(lib.rzk_batch_autotune(ctx.h, jobs, len(jobs), max_probe_jobs, ctypes.byref(v), ctypes.byref(c),
-                                 ctypes.byref(ms), _stream_ptr(stream)), "rzk_batch_autotune")
+                                 ctypes.byref(ms), probes.ctypes.data, _stream_ptr(stream)), "rzk_batch_autotune")
+    if table:
+        return v.value, c.value, ms.value, probes
     return v.value, c.value, ms.value
 
 
