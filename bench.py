@@ -47,6 +47,11 @@ TRAFFIC_BYTES_PER_LAUNCH = (35.6992 + 57.395968) * 1e6
 # (HBM idle, its ~34 MB working set in L2), so the roofline compares the issue rate it
 # reaches with the SMs' peak of one warp instruction per scheduler per cycle.
 INST_PER_LAUNCH = None
+# The same for the secondary workloads' dominant kernels (one full launch each, same capture
+# recipe; see profiles/): LightSlice's and MRCS's tracing passes and the guided path kernel.
+LS_VIS_INST = None
+MRCS_VIS_INST = None
+GUIDED_INST = None
 
 
 def workload_config():
@@ -187,6 +192,22 @@ def kernels_per_call(fn, capture: bool = True):
     n = graph_kernels(g)
     del g
     return n
+
+
+def issue_roofline(inst, step_s, sm_mhz, kernel, note):
+    """Issue-rate roofline of an instruction-bound kernel: its warp instructions per launch
+    (ncu smsp__inst_executed.sum, recorded in profiles/) over the live step time, against
+    SMs x 4 schedulers x one warp instruction per cycle at the sampled SM clock."""
+    import torch
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    mhz = sm_mhz or 1965.0
+    peak = sms * 4 * mhz * 1e6
+    ach = inst / step_s if inst else None
+    return {"bound": "issue", "unit": "Gwarp-inst/s", "kernel": kernel,
+            "achieved": None if ach is None else ach / 1e9, "peak": peak / 1e9,
+            "frac": None if ach is None else ach / peak, "inst_per_launch": inst,
+            "peak_source": f"{sms} SMs x 4 schedulers x 1 warp instruction per cycle at {mhz:.0f} MHz (sampled)",
+            "note": note}
 
 
 def cpu_scene_inputs(sc):
@@ -714,6 +735,35 @@ def run_mrcs(args):
     launches_step = kernels_per_call(step)
     ms = 1e3 * sum(times) / len(times)
     evals = cam.n_pixels * n_reps
+    clk_sum = clk.summary()
+    roofline = issue_roofline(MRCS_VIS_INST, ms / 1e3, clk_sum["sm_mhz"], "mrcs_vis_kernel",
+                              "the tracing pass's warp instructions over the whole clustered-gather step")
+    # CPU baseline: the reference's own MatrixRowColumnSampling (initialize, then
+    # gather_clusters per pixel) run twice on seeded pixel samples of two sizes; the
+    # difference isolates gather_clusters' cost per pixel x representative (the reference
+    # is single-threaded: one global random stream)
+    cpu = {"value": None, "unit": "evals/s", "cores": 1, "kind": "skipped", "sample": ""}
+    if not args.skip_cpu:
+        from oracle import RefHarness
+        if RefHarness.available():
+            ref = RefHarness(sc)
+            recv_np = rzk.records_from_device(recv, sg.RECEIVER_DTYPE)
+            order = np.random.default_rng(VPL_SEED + 4).permutation(cam.n_pixels)
+            small = recv_np[np.sort(order[:64])].copy()
+            t0 = time.perf_counter()
+            _, _, r_small, _ = ref.mrcs(vpls_np, rzk.CLAMP_RADIANCE, tau, VPL_SEED, small)
+            t_small = time.perf_counter() - t0
+            k = int(min(cam.n_pixels, 2048))
+            big = recv_np[np.sort(order[:k])].copy()
+            t0 = time.perf_counter()
+            _, _, r_big, _ = ref.mrcs(vpls_np, rzk.CLAMP_RADIANCE, tau, VPL_SEED, big)
+            t_big = time.perf_counter() - t0
+            reps_ref = int((r_big >= 0).sum())
+            if t_big > t_small:
+                cpu = {"value": (k - 64) * reps_ref / (t_big - t_small), "unit": "evals/s", "cores": 1,
+                       "kind": "reference",
+                       "sample": f"gather_clusters of {k} vs 64 seeded pixels x {reps_ref} representatives "
+                                 f"(initialize included in both runs and cancelled)"}
     line = {
         "metric": "MRCS clustered-gather evals/s (pixel x cluster representative, shadow ray each)",
         "value": evals / (ms / 1e3), "unit": "evals/s", "n_gpus": 1, "steps": len(times),
@@ -726,7 +776,8 @@ def run_mrcs(args):
         "setup_s": setup_s,
         "setup_stage_ms": dict(zip(["pixels_and_columns", "reduced_matrix", "clustering", "representatives"],
                                    info["stage_ms"])),
-        "clocks": clk.summary(), "gpu_launches": launches_step * len(times),
+        "clocks": clk_sum, "roofline": roofline, "cpu_baseline": cpu,
+        "gpu_launches": launches_step * len(times),
         "gpu_launches_note": f"{launches_step} kernels per step, counted as the kernel nodes of one captured step",
         "image_finite": bool(torch.isfinite(out).all()), "tau": tau,
     }
@@ -793,6 +844,41 @@ def run_lightslice(args):
     ms = 1e3 * sum(times) / len(times)
     stages = dict(zip(["points_and_filter", "slicing", "reduced_matrix", "global_clustering",
                        "refinement", "maps", "tables"], info["ms"][:7]))
+    clk_sum = clk.summary()
+    roofline = issue_roofline(LS_VIS_INST, ms / 1e3, clk_sum["sm_mhz"], "cluster_vis_kernel",
+                              "the tracing pass's warp instructions over the whole clustered-gather step")
+    # CPU baseline: the reference's own LightSlice::gather_clusters on all host cores, on a
+    # seeded sample of pixels, from the reference's refinement of the device's reduced matrix
+    # and global clusters (the stages pinned bit-exact by the parity tests)
+    cpu = {"value": None, "unit": "evals/s", "cores": os.cpu_count() or 1, "kind": "skipped", "sample": ""}
+    parity = None
+    if not args.skip_cpu:
+        from oracle import RefHarness, column_magnitudes
+        if RefHarness.available():
+            ref = RefHarness(sc)
+            rls = ref.lightslice(1024, 32, VPL_SEED)
+            rls.set_vpls(vpls_np)
+            R, V, _ = ls.matrix()
+            R, V = R.cpu().numpy(), V.cpu().numpy()
+            g_rep, g_w, assign = ls.global_clusters()
+            rls.refine(R, V, g_rep, g_w, assign, column_magnitudes(R), 2000, VPL_SEED)
+            recv_np = rzk.records_from_device(recv, sg.RECEIVER_DTYPE)
+            order = np.random.default_rng(VPL_SEED + 2).permutation(cam.n_pixels)
+            threads = os.cpu_count() or 1
+            cal = order[:256]
+            t0 = time.perf_counter()
+            rls.gather(recv_np[np.sort(cal)].copy(), rzk.CLAMP_RADIANCE, tau, threads=threads)
+            per = max(time.perf_counter() - t0, 1e-3) / len(cal)
+            pick = np.sort(order[:int(min(cam.n_pixels, max(threads, 10.0 / per)))])
+            t0 = time.perf_counter()
+            exp = rls.gather(recv_np[pick].copy(), rzk.CLAMP_RADIANCE, tau, threads=threads)
+            dt = time.perf_counter() - t0
+            s_evals = int(counts[slice_of[pick][slice_of[pick] >= 0]].sum())
+            cpu = {"value": s_evals / dt, "unit": "evals/s", "cores": threads, "kind": "reference",
+                   "sample": f"{len(pick)} seeded pixels x their slices' clusters ({s_evals} evaluations)"}
+            got = out.cpu().numpy()[pick] * np.float32(num_emitted)
+            parity = {"rel_l2_vs_reference": float(np.linalg.norm(got - exp) / max(np.linalg.norm(exp), 1e-30)),
+                      "sample": f"{len(pick)} pixels of the timed image against the reference's gather_clusters"}
     line = {
         "metric": "LightSlice clustered-gather evals/s (pixel x slice-cluster representative, shadow ray each)",
         "value": evals / (ms / 1e3), "unit": "evals/s", "n_gpus": 1, "steps": len(times),
@@ -804,7 +890,8 @@ def run_lightslice(args):
                    "evals_per_step": evals, "max_slice_size": 1024, "num_clusters": 1000,
                    "max_slice_clusters": 2000, "neighbor_slices": 32,
                    "l2": "flushed between timed steps (256 MiB write)"},
-        "build_s": build_s, "build_stage_ms": stages, "clocks": clk.summary(),
+        "build_s": build_s, "build_stage_ms": stages, "clocks": clk_sum, "roofline": roofline,
+        "cpu_baseline": cpu, "parity": parity,
         "gpu_launches": None if launches_step is None else launches_step * len(times),
         "gpu_launches_note": (f"{launches_step} kernels per step, counted by the CUDA activity profiler over one step"
                               if launches_step else "not counted: the CUDA activity profiler recorded nothing"),
@@ -871,6 +958,43 @@ def run_guided(args):
     launches_step = kernels_per_call(step)
     ms = 1e3 * sum(times) / len(times)
     paths = cam.n_pixels * spp
+    clk_sum = clk.summary()
+    roofline = issue_roofline(GUIDED_INST if (side, spp, args.sampler) == (1024, 16, "jensen") else None,
+                              ms / 1e3, clk_sum["sm_mhz"], "guided_kernel",
+                              "the path kernel's warp instructions over the whole frame (chains and per-pixel mean "
+                              "included in the time)")
+    # CPU baseline: the reference's own tracer (trace_wellington with the same LightSlice
+    # state, rebuilt by the reference's refinement from the device's reduced matrix and
+    # global clusters) on a seeded sample of pixels; one host thread, because the reference
+    # draws every path from its one global random stream
+    cpu = {"value": None, "unit": "paths/s", "cores": 1, "kind": "skipped", "sample": ""}
+    parity = None
+    if not args.skip_cpu:
+        from oracle import RefHarness, column_magnitudes
+        if RefHarness.available():
+            ref = RefHarness(sc)
+            rls = ref.lightslice(args.slice_size, 32, VPL_SEED)
+            rls.set_vpls(rzk.records_from_device(vt, sg.VPL_DTYPE))
+            R, V, _ = ls.matrix()
+            R, V = R.cpu().numpy(), V.cpu().numpy()
+            g_rep, g_w, assign = ls.global_clusters()
+            rls.refine(R, V, g_rep, g_w, assign, column_magnitudes(R), args.max_slice_clusters, VPL_SEED)
+            order = np.random.default_rng(VPL_SEED + 3).permutation(cam.n_pixels)
+            t0 = time.perf_counter()
+            rls.guided(np.sort(order[:16]).astype(np.int32), spp, 8, rr_depth=3, rr_prob=0.5, seed=VPL_SEED,
+                       sampler=args.sampler)
+            per = max(time.perf_counter() - t0, 1e-3) / 16
+            pick = np.sort(order[:int(min(cam.n_pixels, max(16, 10.0 / per)))]).astype(np.int32)
+            t0 = time.perf_counter()
+            want = rls.guided(pick, spp, 8, rr_depth=3, rr_prob=0.5, seed=VPL_SEED, sampler=args.sampler)
+            dt = time.perf_counter() - t0
+            cpu = {"value": len(pick) * spp / dt, "unit": "paths/s", "cores": 1, "kind": "reference",
+                   "sample": f"{len(pick)} seeded pixels x {spp} spp"}
+            if args.sampler == "jensen":
+                got = out.cpu().numpy()[pick]
+                m = want.mean(axis=1)
+                parity = {"rel_l2_vs_reference": float(np.linalg.norm(got - m) / max(np.linalg.norm(m), 1e-30)),
+                          "sample": f"{len(pick)} pixels of the timed frame against the reference tracer"}
     line = {
         "metric": ("guided path-tracing paths/s (LightSlice " +
                    ("Jensen-map" if args.sampler == "jensen" else "Metropolis-chain") +
@@ -885,7 +1009,8 @@ def run_guided(args):
                    "slices": info["slices"], "slice_clusters": info["slice_clusters"], "map_resolution": 32,
                    "max_slice_size": args.slice_size,
                    "l2": "flushed between timed steps (256 MiB write)"},
-        "setup_s": setup_s, "lightslice_stage_ms": info["ms"][:7], "clocks": clk.summary(),
+        "setup_s": setup_s, "lightslice_stage_ms": info["ms"][:7], "clocks": clk_sum, "roofline": roofline,
+        "cpu_baseline": cpu, "parity": parity,
         "gpu_launches": launches_step * len(times),
         "gpu_launches_note": f"{launches_step} kernels per step, counted as the kernel nodes of one captured step",
         "image_finite": bool(torch.isfinite(out).all()), "image_mean": float(out.mean()),

@@ -284,6 +284,7 @@ class RefHarness:
             L.rref_ls_clusters.argtypes = [P, P, P, P, P, P, P, P, P, P, P]
             L.rref_ls_maps.argtypes = [P, P, P, P, P]
             L.rref_ls_gather.argtypes = [P, P, I32, I32, F32, P]
+            L.rref_ls_gather_mt.argtypes = [P, P, I32, I32, F32, P, I32]
             L.rref_ls_guided.argtypes = [P, P, I32, I32, I32, I32, F32, I32, U32, P]
             L.rref_ls_density.argtypes = [P, P, P, I32, P]
             L.rref_ls_set_sampler.argtypes = [P, I32]
@@ -561,10 +562,13 @@ class RefLightSlice:
         RefHarness.lib().rref_ls_maps(self.h, _ptr(m), _ptr(v), _ptr(sm), _ptr(pr))
         return {"maps": m, "valid": v, "sum": sm, "prob": pr}
 
-    def gather(self, recv, clamp_mode, tau):
+    def gather(self, recv, clamp_mode, tau, threads=1):
         recv = np.ascontiguousarray(recv)
         out = np.zeros((len(recv), 3), np.float32)
-        RefHarness.lib().rref_ls_gather(self.h, _ptr(recv), len(recv), clamp_mode, tau, _ptr(out))
+        if threads > 1:
+            RefHarness.lib().rref_ls_gather_mt(self.h, _ptr(recv), len(recv), clamp_mode, tau, _ptr(out), threads)
+        else:
+            RefHarness.lib().rref_ls_gather(self.h, _ptr(recv), len(recv), clamp_mode, tau, _ptr(out))
         return out
 
 

@@ -602,4 +602,25 @@ void rref_ls_gather(void *hp, const rzk_receiver *recv, int n, int mode, float t
     }
 }
 
+/* The same on n_threads host threads over the receivers (gather_clusters only reads the
+ * LightSlice state, the scene and the evaluator's clamp settings). */
+void rref_ls_gather_mt(void *hp, const rzk_receiver *recv, int n, int mode, float tau, float *out, int n_threads) {
+    RefLs *h = (RefLs *)hp;
+    h->ev.mode = mode;
+    h->ev.tau = tau;
+    if (n_threads < 1) n_threads = 1;
+    auto work = [&](int t) {
+        const int i0 = (int)((long long)n * t / n_threads), i1 = (int)((long long)n * (t + 1) / n_threads);
+        for (int i = i0; i < i1; ++i) {
+            Receiver r = to_receiver(h->s, recv[i]);
+            Rgb L = h->ls->gather_clusters(r, &h->ev);
+            put3(out + 3 * i, L);
+        }
+    };
+    std::vector<std::thread> th;
+    for (int t = 1; t < n_threads; ++t) th.emplace_back(work, t);
+    work(0);
+    for (auto &x : th) x.join();
+}
+
 }  // extern "C"

@@ -133,6 +133,36 @@ __device__ __forceinline__ bool pair_survives(const RecvRegs &r, const rzk_vpl &
     return true;
 }
 
+// A cheaper first test that implies pair_survives' "exactly zero" answer: no division or
+// square root.  It returns true only where G and the power are certainly finite and one of
+// the BRDF early-outs certainly fires: the receiver sees its surface from behind or the VPL
+// was reached from behind its surface (the same dot products pair_survives tests, exactly),
+// or the VPL lies behind the receiver's surface / the receiver behind the VPL's, judged on
+// the unnormalised direction d = q - p with a margin: dot(d, n) <= -4e-6 |d| puts the
+// rounded dot(unit(d), n) below -2e-6, under ZERO_EPSILON whatever the rounding of either
+// product (each within ~1e-6 of exact for unit normals).  Pairs it passes go through
+// pair_survives, so the set of surviving pairs is unchanged.
+__device__ __forceinline__ bool pair_clearly_zero(const RecvRegs &r, const rzk_vpl &l) {
+    const V3 d = sub(ld3(l.p), r.p);
+    const float dd = dot(d, d);
+    if (!(dd >= 1e-18f && dd <= 1e30f)) return false;
+    if (!(isfinite(l.contrib[0]) && isfinite(l.contrib[1]) && isfinite(l.contrib[2]))) return false;
+    // G = |d1 d2| / dd^2 finite: d1 d2 finite and at most 1e30 dd^2
+    const float g = dot(r.ns, d) * dot(ld3(l.n), d);
+    if (!(fabsf(g) <= dd * dd * 1e30f)) return false;
+    if (dot(r.wo, r.uvn.n) <= ZERO_EPSILON) return true;
+    const float m2 = 1.6e-11f * dd;   // (4e-6)^2 |d|^2
+    const float a = dot(d, r.uvn.n);
+    if (a < 0.0f && a * a >= m2) return true;
+    if (l.mat >= 0) {
+        const V3 lnn = ld3(l.nn);
+        if (dot(ld3(l.wi), lnn) <= ZERO_EPSILON) return true;
+        const float b = dot(d, lnn);
+        if (b > 0.0f && b * b >= m2) return true;
+    }
+    return false;
+}
+
 __device__ __forceinline__ Rgb pair_radiance(const DevScene &s, const RecvRegs &r, const rzk_material &rm,
                                              const rzk_vpl &l, const PairGeo &pg, int mode, float tau) {
     Rgb sb = brdf_eval(rm, r.uvn, r.wo, pg.wi);
@@ -361,6 +391,7 @@ __device__ __forceinline__ bool gather_item(const DevScene &s, const rzk_receive
         const int cnt = min(TILE, j1 - (j0 + k * TILE));
         for (int v = 0; v < cnt; ++v) {
             const rzk_vpl &l = tile[v];
+            if (!__any_sync(kFull, active && !pair_clearly_zero(r, l))) continue;
             PairGeo pg;
             bool act = active && pair_survives(r, l, pg);
             const unsigned am = __ballot_sync(kFull, act);
@@ -429,7 +460,7 @@ __device__ __forceinline__ bool visibility_item(const DevScene &s, const rzk_rec
         for (int v = 0; v < cnt; ++v) {
             const rzk_vpl &l = tile[v];
             PairGeo pg;
-            bool act = active && pair_survives(r, l, pg);
+            bool act = active && !pair_clearly_zero(r, l) && pair_survives(r, l, pg);
             unsigned vis = 0u;
             const unsigned am = __ballot_sync(kFull, act);
             n_rays += (unsigned)__popc(am);
