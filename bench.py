@@ -46,12 +46,12 @@ TRAFFIC_BYTES_PER_LAUNCH = (35.6992 + 57.395968) * 1e6
 # the same one-pass capture, recorded in profiles/): the gather is instruction-issue bound
 # (HBM idle, its ~34 MB working set in L2), so the roofline compares the issue rate it
 # reaches with the SMs' peak of one warp instruction per scheduler per cycle.
-INST_PER_LAUNCH = None
+INST_PER_LAUNCH = 94289616557
 # The same for the secondary workloads' dominant kernels (one full launch each, same capture
 # recipe; see profiles/): LightSlice's and MRCS's tracing passes and the guided path kernel.
-LS_VIS_INST = None
-MRCS_VIS_INST = None
-GUIDED_INST = None
+LS_VIS_INST = 8180280706
+MRCS_VIS_INST = 1554548976
+GUIDED_INST = 422341967193
 
 
 def workload_config():

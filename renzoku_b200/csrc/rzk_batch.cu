@@ -87,8 +87,8 @@ __global__ void batch_reduce_kernel(const __grid_constant__ JobTable t) {
     const BatchJob &jb = t.jobs[j];
     const long long k = i - jb.out_begin;
     const long long stride = 3LL * jb.n_recv;
-    float acc = jb.partial[k];
-    for (int c = 1; c < jb.n_chunks; ++c) acc += jb.partial[(size_t)c * stride + k];
+    float acc = __ldcs(jb.partial + k);   // read once: evict-first
+    for (int c = 1; c < jb.n_chunks; ++c) acc += __ldcs(jb.partial + (size_t)c * stride + k);
     jb.out[k] = acc * jb.scale;
 }
 

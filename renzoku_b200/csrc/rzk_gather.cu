@@ -398,8 +398,8 @@ __global__ void reduce_chunks_kernel(const float *partial, int n_recv, int n_chu
                                      float *out) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= 3 * n_recv) return;
-    float acc = partial[i];
-    for (int c = 1; c < n_chunks; ++c) acc += partial[(size_t)c * 3 * n_recv + i];
+    float acc = __ldcs(partial + i);   // read once: evict-first
+    for (int c = 1; c < n_chunks; ++c) acc += __ldcs(partial + (size_t)c * 3 * n_recv + i);
     out[i] = acc * scale;
 }
 

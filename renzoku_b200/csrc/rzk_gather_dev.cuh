@@ -361,8 +361,10 @@ __device__ __forceinline__ bool gather_item(const DevScene &s, const rzk_receive
     // empty chunk must not arm a barrier phase that no wait consumes)
     if (n_tiles <= 0 || !__any_sync(kFull, active)) {
         if (ri >= 0) {
+            // partial sums are read once by the chunk reduction: streaming stores keep them
+            // from displacing the traversal working set in L2
             float *o = partial + 3 * ((size_t)chunk * n_recv + ri);
-            o[0] = 0.0f; o[1] = 0.0f; o[2] = 0.0f;
+            __stcs(o, 0.0f); __stcs(o + 1, 0.0f); __stcs(o + 2, 0.0f);
         }
         return true;
     }
@@ -408,7 +410,7 @@ __device__ __forceinline__ bool gather_item(const DevScene &s, const rzk_receive
     if (lane == 0 && s.rays && n_rays) atomicAdd(s.rays, n_rays);
     if (ri >= 0) {
         float *o = partial + 3 * ((size_t)chunk * n_recv + ri);
-        o[0] = sum.r; o[1] = sum.g; o[2] = sum.b;
+        __stcs(o, sum.r); __stcs(o + 1, sum.g); __stcs(o + 2, sum.b);
     }
     return true;
 }
