@@ -547,7 +547,10 @@ def run_batch(args):
     rbuild.build()
     from renzoku_b200 import instances as im, rzk
     ctx = rzk.Context(0)
-    specs = im.batch_specs(args.instances, seed=2024)
+    if args.small:   # many small instances, where per-launch ramp and tail matter most
+        specs = im.batch_specs(args.instances, seed=2024, tris=(10_000, 50_000), side=(64, 256), vpls=(1_000, 4_000))
+    else:
+        specs = im.batch_specs(args.instances, seed=2024)
     t0 = time.perf_counter()
     insts = [im.make_instance(ctx, s) for s in specs]
     setup_s = time.perf_counter() - t0
@@ -609,7 +612,7 @@ def run_batch(args):
         "value": evals / mg, "unit": "evals/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * mg, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"batched_gather_{len(insts)}_instances_seed2024",
+        "config": {"workload": f"batched_gather_{len(insts)}_{'small_' if args.small else ''}instances_seed2024",
                    "instances": len(insts), "evals_per_step": evals,
                    "triangles": [i.agg.n_tris for i in insts],
                    "image_sides": [i.spec.width for i in insts], "vpls": [i.n_vpl for i in insts],
@@ -1202,6 +1205,8 @@ def main():
                          "(0 leaves the sweep out)")
     ap.add_argument("--budget-gb", type=float, default=4.0, help="serve: HBM admission budget")
     ap.add_argument("--instances", type=int, default=64)
+    ap.add_argument("--small", action="store_true",
+                    help="batch: small instances (10k-50k triangles, 64^2-256^2 images, 1k-4k VPLs)")
     ap.add_argument("--vpls", type=int, default=0,
                     help="scaled: VPL count (default 32,768; smaller for profiling captures)")
     ap.add_argument("--skip-cpu", action="store_true",
