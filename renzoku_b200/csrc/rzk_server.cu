@@ -8,14 +8,17 @@
 // for it; otherwise the call returns RZK_ERR_BUSY at once and the caller decides whether to
 // retry.
 //
-// One worker thread owns a context and two streams ("lanes"): gathers run on one, guided
-// renders on the other, so the two kinds of work overlap on the device - a guided render's
-// paths fill the SMs a finishing gather frees and the reverse.  Each lane keeps at most two
-// launch groups queued on its stream (one running, one behind it, so the GPU never waits for
-// the host).  Whenever a lane has room the worker issues its next group from the requests
-// not yet launched, in arrival order: on the gather lane every waiting gather, oldest first,
-// as ONE persistent batched launch of at most ~2e9 evaluations (a request larger than that
-// goes alone); on the guided lane the oldest guided render.  Continuous batching: a request
+// One worker thread owns a context and four streams ("lanes"): gathers run on one, guided
+// renders on the other three, so the kinds of work overlap on the device - a guided
+// render's paths fill the SMs a finishing gather frees and the reverse, and small guided
+// renders (a few thousand paths, far fewer than the GPU holds) run side by side.  The
+// gather lane keeps at most two launch groups queued on its stream (one running, one behind
+// it, so the GPU never waits for the host), each guided lane one.  Whenever a lane has room
+// the worker issues its next group from the requests not yet launched, in arrival order: on
+// the gather lane every waiting gather, oldest first, as ONE persistent batched launch of
+// at most ~2e9 evaluations (a request larger than that goes alone); on a guided lane the
+// oldest guided render (Metropolis renders only on the first guided lane: their chain pool
+// is the context's scratch).  Continuous batching: a request
 // that arrives while others run joins the lane's very next group.  A host function after a
 // group's last kernel marks its requests done.  With batching off the worker issues one
 // request at a time in arrival order, with its own launches, on one stream (the plain
@@ -40,7 +43,7 @@ double now_ms() {
 }
 
 enum { kQueued = 0, kRunning = 1, kDone = 2, kCancelled = 3, kFailed = 4 };
-enum { kLaneGather = 0, kLaneGuided = 1, kLanes = 2 };
+enum { kLaneGather = 0, kLaneGuided = 1, kGuidedLanes = 3, kLanes = 1 + kGuidedLanes };
 
 struct Req {
     uint64_t id = 0;
@@ -55,7 +58,8 @@ struct Req {
 };
 
 constexpr double kLaunchCost = 2e9;     // work of one batched launch (~30 ms of gather)
-constexpr int kMaxInFlight = 2;         // launch groups per lane: one running, one queued
+constexpr int kMaxInFlight = 2;         // launch groups on the gather lane: one running, one queued
+constexpr int kGuidedInFlight = 1;      // per guided lane (concurrency comes from the lanes)
 constexpr int64_t kFreeReserve = 256ll << 20;   // device memory never handed to requests
 constexpr size_t kTimingCap = 1 << 20;  // completed requests whose timings are kept
 
@@ -69,7 +73,7 @@ int default_chunks(int n_vpl) {   // rzk_gather's automatic chunk count
 struct rzk_server {
     int device = 0;
     rzk_context *ctx = nullptr;
-    cudaStream_t st[kLanes] = {nullptr, nullptr};
+    cudaStream_t st[kLanes] = {};
     rzk_server_params prm{};
     int64_t budget = 0, held = 0, free_bytes = 0;
     int64_t n_submitted = 0, n_rejected = 0, n_completed = 0, n_launches = 0;
@@ -79,7 +83,7 @@ struct rzk_server {
     std::condition_variable cv_work, cv_done;
     std::deque<Req *> queue;     // submitted, not yet seen by the worker
     std::vector<Req *> ready;    // seen by the worker, not yet launched (arrival order)
-    int in_flight[kLanes] = {0, 0};   // launch groups issued and not finished, per lane
+    int in_flight[kLanes] = {};   // launch groups issued and not finished, per lane
     std::unordered_map<uint64_t, Req *> reqs;
     // per completed request: kind, queue wait (submit -> launch) and run (launch -> done), ms
     std::vector<int32_t> t_kind;
@@ -203,9 +207,22 @@ void launch_group(rzk_server *s, Group *g) {
     }
 }
 
-int lane_of(const rzk_server *s, const Req *q) {
-    if (!s->prm.batching) return kLaneGather;   // the plain loop: one stream
-    return q->r.kind == RZK_REQ_GUIDED ? kLaneGuided : kLaneGather;
+int lane_cap(int lane) { return lane == kLaneGather ? kMaxInFlight : kGuidedInFlight; }
+
+// Whether a lane may run a request: the plain loop runs everything on the gather lane; with
+// batching gathers take the gather lane, Jensen renders any guided lane, Metropolis renders
+// the first one.
+bool lane_takes(const rzk_server *s, int lane, const Req *q) {
+    if (!s->prm.batching) return lane == kLaneGather;
+    if (q->r.kind != RZK_REQ_GUIDED) return lane == kLaneGather;
+    if (lane == kLaneGather) return false;
+    return q->r.sampler != RZK_GUIDE_METROPOLIS || lane == kLaneGuided;
+}
+
+bool can_launch(const rzk_server *s, const Req *q) {
+    for (int lane = 0; lane < kLanes; ++lane)
+        if (s->in_flight[lane] < lane_cap(lane) && lane_takes(s, lane, q)) return true;
+    return false;
 }
 
 // Picks the next group for a lane with room (called with the lock held), or nullptr.
@@ -223,13 +240,13 @@ Group *next_group(rzk_server *s) {
         rd.erase(rd.begin());
         return g;
     }
-    for (int lane : {kLaneGather, kLaneGuided}) {
-        if (s->in_flight[lane] >= kMaxInFlight) continue;
-        const int max_batch = lane == kLaneGuided ? 1 : (s->prm.max_batch > 0 ? s->prm.max_batch : 256);
+    for (int lane = 0; lane < kLanes; ++lane) {
+        if (s->in_flight[lane] >= lane_cap(lane)) continue;
+        const int max_batch = lane != kLaneGather ? 1 : (s->prm.max_batch > 0 ? s->prm.max_batch : 256);
         std::vector<Req *> take;
         double cost = 0.0;
         for (Req *q : rd) {
-            if (lane_of(s, q) != lane) continue;
+            if (!lane_takes(s, lane, q)) continue;
             if (!take.empty() && ((int)take.size() >= max_batch || cost + q->cost > kLaunchCost)) break;
             take.push_back(q);
             cost += q->cost;
@@ -265,7 +282,7 @@ void worker_main(rzk_server *s) {
                 }
                 if (s->ready.empty()) return s->stop;
                 for (Req *q : s->ready)
-                    if (s->in_flight[lane_of(s, q)] < kMaxInFlight) return true;
+                    if (can_launch(s, q)) return true;
                 return false;
             });
             if (s->ready.empty()) break;   // stopping and drained
