@@ -38,10 +38,11 @@ VPL_PARTICLES = 24000
 MAX_BOUNCE = 3
 TAU_PAIRS = 65536
 # DRAM bytes (read + write) of one full gather launch of this workload, from the one-pass
-# capture `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum -k regex:gather_persistent
-# -s 3 -c 1 python bench.py --steps 1 --warmup 3 --skip-cpu` (35.70 MB read, 57.40 MB
-# written; the writes are the per-chunk partial sums), recorded in profiles/.
-TRAFFIC_BYTES_PER_LAUNCH = (35.6992 + 57.395968) * 1e6
+# capture `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum --clock-control none
+# -k regex:gather_persistent -s 3 -c 1 python bench.py --steps 1 --warmup 3 --skip-cpu
+# --serve-duration 0` (36.48 MB read, 55.29 MB written; the writes are the per-chunk partial
+# sums), recorded in profiles/.
+TRAFFIC_BYTES_PER_LAUNCH = (36.48 + 55.29) * 1e6
 # Warp instructions of one full gather launch of this workload (smsp__inst_executed.sum from
 # the same one-pass capture, recorded in profiles/): the gather is instruction-issue bound
 # (HBM idle, its ~34 MB working set in L2), so the roofline compares the issue rate it
