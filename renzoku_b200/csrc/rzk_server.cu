@@ -12,8 +12,13 @@
 // renders on the other three, so the kinds of work overlap on the device - a guided
 // render's paths fill the SMs a finishing gather frees and the reverse, and small guided
 // renders (a few thousand paths, far fewer than the GPU holds) run side by side.  The
-// gather lane keeps at most two launch groups queued on its stream (one running, one behind
-// it, so the GPU never waits for the host), each guided lane one.  Whenever a lane has room
+// gather lane and the first guided lane have the device's highest stream priority, the
+// other two guided lanes its lowest: the oldest guided render takes the first guided lane
+// and its blocks are scheduled ahead of the younger renders', which only backfill SMs it
+// leaves idle, so it finishes about as fast as it would alone (guided renders use the
+// one-thread-per-path kernel here, whose short blocks let the priorities act as SMs free
+// up).  The gather lane keeps at most two launch groups queued on its stream (one running,
+// one behind it, so the GPU never waits for the host), each guided lane one.  Whenever a lane has room
 // the worker issues its next group from the requests not yet launched, in arrival order: on
 // the gather lane every waiting gather, oldest first, as ONE persistent batched launch of
 // at most ~2e9 evaluations (a request larger than that goes alone); on a guided lane the
@@ -154,7 +159,8 @@ void launch_group(rzk_server *s, Group *g) {
                 q->status = RZK_ERR_NOMEM;
                 continue;
             }
-            rzk_guided_params gp{r.spp, r.max_bounce, r.rr_depth, r.rr_prob, 1, r.seed, r.sampler, 0};
+            // short blocks (one thread per path) so that the lanes' stream priorities act
+            rzk_guided_params gp{r.spp, r.max_bounce, r.rr_depth, r.rr_prob, 1, r.seed, r.sampler, 0, 1};
             q->status = rzk_guided_render(s->ctx, r.scene, r.lightslice, &r.camera, &gp, r.d_rgb, q->d_paths, st);
             g->launches += r.sampler == RZK_GUIDE_METROPOLIS ? 3 : 2;   // (chains +) path kernel + per-pixel mean
         } else if (!s->prm.batching) {
@@ -317,8 +323,11 @@ rzk_status rzk_server_create(int device, const rzk_server_params *params, rzk_se
         delete s;
         return r;
     }
-    for (cudaStream_t &st : s->st)
-        if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+    int prio_least = 0, prio_greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest);
+    for (int lane = 0; lane < kLanes; ++lane)
+        if (cudaStreamCreateWithPriority(&s->st[lane], cudaStreamNonBlocking,
+                                         lane <= kLaneGuided ? prio_greatest : prio_least) != cudaSuccess) {
             for (cudaStream_t x : s->st)
                 if (x) cudaStreamDestroy(x);
             rzk_context_destroy(s->ctx);
