@@ -52,7 +52,7 @@ INST_PER_LAUNCH = 94289616557
 # recipe; see profiles/): LightSlice's and MRCS's tracing passes and the guided path kernel.
 LS_VIS_INST = 8180280706
 MRCS_VIS_INST = 1554548976
-GUIDED_INST = {1: 422341967193, 0: None}   # by path kernel: 1 one thread per path, 0 persistent
+GUIDED_INST = 422341967193
 
 
 def workload_config():
@@ -945,8 +945,7 @@ def run_guided(args):
     spp = args.spp
 
     def step():
-        ls.guided_render(cam, spp, 8, rr_depth=3, rr_prob=0.5, seed=VPL_SEED, out=out, sampler=args.sampler,
-                         path_kernel=args.path_kernel)
+        ls.guided_render(cam, spp, 8, rr_depth=3, rr_prob=0.5, seed=VPL_SEED, out=out, sampler=args.sampler)
 
     for _ in range(args.warmup):
         step()
@@ -967,8 +966,7 @@ def run_guided(args):
     ms = 1e3 * sum(times) / len(times)
     paths = cam.n_pixels * spp
     clk_sum = clk.summary()
-    roofline = issue_roofline(GUIDED_INST[args.path_kernel] if (side, spp, args.sampler) == (1024, 16, "jensen")
-                              else None,
+    roofline = issue_roofline(GUIDED_INST if (side, spp, args.sampler) == (1024, 16, "jensen") else None,
                               ms / 1e3, clk_sum["sm_mhz"], "guided_kernel",
                               "the path kernel's warp instructions over the whole frame (chains and per-pixel mean "
                               "included in the time)")
@@ -1013,7 +1011,7 @@ def run_guided(args):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"guided_pt_room_spheres_{agg.n_tris}_tris_{side}x{side}_{spp}spp_depth8_rr3"
                                + ("" if args.sampler == "jensen" else "_metropolis"),
-                   "sampler": args.sampler, "path_kernel": args.path_kernel, "triangles": agg.n_tris, "spp": spp, "max_bounce": 8, "rr_depth": 3, "rr_prob": 0.5,
+                   "sampler": args.sampler, "triangles": agg.n_tris, "spp": spp, "max_bounce": 8, "rr_depth": 3, "rr_prob": 0.5,
                    "vpls": n_vpl, "vpls_used": info["vpls_used"], "global_clusters": info["global_clusters"],
                    "slices": info["slices"], "slice_clusters": info["slice_clusters"], "map_resolution": 32,
                    "max_slice_size": args.slice_size,
@@ -1202,8 +1200,6 @@ def main():
     ap.add_argument("--sampler", choices=["jensen", "metropolis"], default="jensen",
                     help="guided: LightSlice's direction sampler")
     ap.add_argument("--side", type=int, default=1024)
-    ap.add_argument("--path-kernel", type=int, default=0, choices=[0, 1],
-                    help="guided: 0 persistent grid-stride path kernel, 1 one thread per path")
     ap.add_argument("--max-slice-clusters", type=int, default=4096)
     ap.add_argument("--slice-size", type=int, default=4096)
     ap.add_argument("--rates", default=SERVE_RATES, help="serve: arrival rates (req/s)")

@@ -560,9 +560,6 @@ typedef struct {
                                  RZK_GUIDE_METROPOLIS (1, the reference's default) */
     int32_t chain_samples;    /* METROPOLIS: chain states kept per slice after the warm-up
                                  (0: 4096) */
-    int32_t path_kernel;      /* 0: persistent threads taking paths in a grid-stride loop (a lane
-                                 whose path ended starts the next); 1: one thread per path.
-                                 Same image either way. */
 } rzk_guided_params;
 enum { RZK_GUIDE_JENSEN = 0, RZK_GUIDE_METROPOLIS = 1 };
 

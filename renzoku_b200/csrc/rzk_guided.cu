@@ -196,44 +196,27 @@ __device__ Rgb trace_path(const DevScene &s, const GuideDev &G, const PtParams &
     return value;
 }
 
-// Sample s of pixel k is path k * spp + s, so neighbouring threads share a pixel (and their
-// first hit).  PERSIST: the grid holds only as many threads as the SMs keep resident and
-// each thread takes paths in a grid-stride loop, so a lane whose path ended early starts
-// its next path instead of idling until the warp's longest path ends (paths differ in
-// length by the technique draws, roulette and escapes); otherwise one thread per path.  A
-// path's value depends only on its index, so both give the same image.
-template <bool METRO, bool PERSIST>
+// one thread per path: sample s of pixel k is path k * spp + s, so neighbouring threads
+// share a pixel (and their first hit)
+template <bool METRO>
 __global__ void __launch_bounds__(kPtBlock) guided_kernel(DevScene s, GuideDev G, PtParams P, float *paths) {
     __shared__ int stack_mem[STACK_CAP * kPtBlock];
+    const long long path = (long long)blockIdx.x * kPtBlock + threadIdx.x;
     const int W = P.cam.width, H = P.cam.height;
-    const long long n_paths = (long long)W * H * P.spp;
-    const long long stride = PERSIST ? (long long)gridDim.x * kPtBlock : n_paths;
+    if (path >= (long long)W * H * P.spp) return;
     Stack<kPtBlock> stk;
     stk.init(stack_mem + threadIdx.x);
-    for (long long path = (long long)blockIdx.x * kPtBlock + threadIdx.x; path < n_paths; path += stride) {
-        const int k = (int)(path / P.spp);
-        const int i = k / W, j = k - i * W;
-        Rng g;
-        g.init(P.seed, 6u, (uint32_t)path);
-        Ray ray = camera_ray(P.cam, i, j);
-        HitGeo h;
-        Rgb L = crgb(0.0f, 0.0f, 0.0f);
-        if (trace_closest(s, ray, stk, h))
-            L = trace_path<kPtBlock, METRO>(s, G, P, to_recv(h, ray), h.light, g, stk);
-        paths[3 * path] = L.r;
-        paths[3 * path + 1] = L.g;
-        paths[3 * path + 2] = L.b;
-    }
-}
-
-// Resident blocks of a path kernel on the current device (its occupancy x SMs).
-template <bool METRO>
-unsigned resident_blocks() {
-    int dev = 0, sms = 0, per_sm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, guided_kernel<METRO, true>, kPtBlock, 0);
-    return (unsigned)std::max(1, sms * std::max(1, per_sm));
+    const int k = (int)(path / P.spp);
+    const int i = k / W, j = k - i * W;
+    Rng g;
+    g.init(P.seed, 6u, (uint32_t)path);
+    Ray ray = camera_ray(P.cam, i, j);
+    HitGeo h;
+    Rgb L = crgb(0.0f, 0.0f, 0.0f);
+    if (trace_closest(s, ray, stk, h)) L = trace_path<kPtBlock, METRO>(s, G, P, to_recv(h, ray), h.light, g, stk);
+    paths[3 * path] = L.r;
+    paths[3 * path + 1] = L.g;
+    paths[3 * path + 2] = L.b;
 }
 
 // eval_incoming_radiance of slice s at (x, y), the slice's points split over the warp's lanes
@@ -379,7 +362,7 @@ rzk_status rzk_guided_render(rzk_context *ctx, rzk_scene *scene, rzk_lightslice 
     if (q.spp <= 0 || q.max_bounce < 1 || q.max_bounce > kMaxBounce || q.rr_depth < 0 ||
         (q.rr_depth > 0 && !(q.rr_prob > 0.0f && q.rr_prob <= 1.0f)) || cam->width <= 0 || cam->height <= 0 ||
         (q.sampler != RZK_GUIDE_JENSEN && q.sampler != RZK_GUIDE_METROPOLIS) || q.chain_samples < 0 ||
-        q.chain_samples > (1 << 24) || q.path_kernel < 0 || q.path_kernel > 1)
+        q.chain_samples > (1 << 24))
         return RZK_ERR_INVALID;
     cudaStream_t st = (cudaStream_t)stream;
     GuideDev G;
@@ -411,15 +394,9 @@ rzk_status rzk_guided_render(rzk_context *ctx, rzk_scene *scene, rzk_lightslice 
             metro_chain_kernel<false><<<dim3(G.n_slices, kChainsPerSlice), 32, 0, st>>>(G, q.seed, pool_n,
                                                                                       (float4 *)ctx->d_partial);
         RZK_CUDA_TRY(cudaGetLastError());
-        if (q.path_kernel == 0)
-            guided_kernel<true, true><<<std::min(blocks, resident_blocks<true>()), kPtBlock, 0, st>>>(scene->dev(), G, P, paths);
-        else
-            guided_kernel<true, false><<<blocks, kPtBlock, 0, st>>>(scene->dev(), G, P, paths);
+        guided_kernel<true><<<blocks, kPtBlock, 0, st>>>(scene->dev(), G, P, paths);
     } else {
-        if (q.path_kernel == 0)
-            guided_kernel<false, true><<<std::min(blocks, resident_blocks<false>()), kPtBlock, 0, st>>>(scene->dev(), G, P, paths);
-        else
-            guided_kernel<false, false><<<blocks, kPtBlock, 0, st>>>(scene->dev(), G, P, paths);
+        guided_kernel<false><<<blocks, kPtBlock, 0, st>>>(scene->dev(), G, P, paths);
     }
     RZK_CUDA_TRY(cudaGetLastError());
     guided_mean_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(paths, (int)n, q.spp, d_rgb);

@@ -15,9 +15,8 @@
 // gather lane and the first guided lane have the device's highest stream priority, the
 // other two guided lanes its lowest: the oldest guided render takes the first guided lane
 // and its blocks are scheduled ahead of the younger renders', which only backfill SMs it
-// leaves idle, so it finishes about as fast as it would alone (guided renders use the
-// one-thread-per-path kernel here, whose short blocks let the priorities act as SMs free
-// up).  The gather lane keeps at most two launch groups queued on its stream (one running,
+// leaves idle, so it finishes about as fast as it would alone (the path kernel's blocks
+// are short - one thread per path - so the priorities act as SMs free up).  The gather lane keeps at most two launch groups queued on its stream (one running,
 // one behind it, so the GPU never waits for the host), each guided lane one.  Whenever a lane has room
 // the worker issues its next group from the requests not yet launched, in arrival order: on
 // the gather lane every waiting gather, oldest first, as ONE persistent batched launch of
@@ -159,8 +158,7 @@ void launch_group(rzk_server *s, Group *g) {
                 q->status = RZK_ERR_NOMEM;
                 continue;
             }
-            // short blocks (one thread per path) so that the lanes' stream priorities act
-            rzk_guided_params gp{r.spp, r.max_bounce, r.rr_depth, r.rr_prob, 1, r.seed, r.sampler, 0, 1};
+            rzk_guided_params gp{r.spp, r.max_bounce, r.rr_depth, r.rr_prob, 1, r.seed, r.sampler, 0};
             q->status = rzk_guided_render(s->ctx, r.scene, r.lightslice, &r.camera, &gp, r.d_rgb, q->d_paths, st);
             g->launches += r.sampler == RZK_GUIDE_METROPOLIS ? 3 : 2;   // (chains +) path kernel + per-pixel mean
         } else if (!s->prm.batching) {

@@ -727,8 +727,7 @@ def lightslice_params(**kw) -> LightSliceParamsC:
 class GuidedParamsC(ctypes.Structure):
     """ctypes mirror of rzk_guided_params."""
     _fields_ = [("spp", I32), ("max_bounce", I32), ("rr_depth", I32), ("rr_prob", F32),
-                ("direct_lighting", I32), ("seed", U32), ("sampler", I32), ("chain_samples", I32),
-                ("path_kernel", I32)]
+                ("direct_lighting", I32), ("seed", U32), ("sampler", I32), ("chain_samples", I32)]
 
 
 GUIDE_JENSEN = 0
@@ -873,7 +872,7 @@ class LightSliceCuda:
 
     def guided_render(self, cam: "Camera", spp: int, max_bounce: int, rr_depth: int = 0, rr_prob: float = 1.0,
                       direct: bool = True, seed: int = 2013, paths: bool = False, out=None, stream=None,
-                      sampler: str = "jensen", chain_samples: int = 0, path_kernel: int = 0):
+                      sampler: str = "jensen", chain_samples: int = 0):
         """LightSlice-guided path tracing (rzk_guided_render) with the "jensen" or "metropolis"
         direction sampler: the per-pixel mean image, and the per-path radiance [W*H, spp, 3]
         when paths=True."""
@@ -883,8 +882,7 @@ class LightSliceCuda:
             out = torch.empty((n, 3), dtype=torch.float32, device="cuda")
         pt = torch.empty((n, spp, 3), dtype=torch.float32, device="cuda") if paths else None
         mode = {"jensen": GUIDE_JENSEN, "metropolis": GUIDE_METROPOLIS}[sampler]
-        prm = GuidedParamsC(spp, max_bounce, rr_depth, rr_prob, 1 if direct else 0, seed, mode, chain_samples,
-                            path_kernel)
+        prm = GuidedParamsC(spp, max_bounce, rr_depth, rr_prob, 1 if direct else 0, seed, mode, chain_samples)
         check(self.lib.rzk_guided_render(self.agg.ctx.h, self.agg.h, self.h, cam.rec.ctypes.data, ctypes.byref(prm),
                                          _dptr(out), _dptr(pt) if pt is not None else None, _stream_ptr(stream)),
               "rzk_guided_render")

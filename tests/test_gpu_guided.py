@@ -67,25 +67,6 @@ def test_guided_paths_match_reference(ctx, oracle_built, rr_depth):
     assert np.all(np.abs(ours.mean(axis=1) - ref.mean(axis=1)) <= 1e-3 * np.abs(ref.mean(axis=1)) + 1e-6)
 
 
-@pytest.mark.parametrize("sampler", ["jensen", "metropolis"])
-def test_guided_path_kernels_agree(ctx, oracle_built, sampler):
-    """The persistent grid-stride path kernel and the one-thread-per-path kernel compute
-    every path from its own stream: the same paths and image, bit for bit."""
-    from oracle import RefHarness
-    if not RefHarness.available():
-        pytest.skip("reference harness not built")
-    sc = sg.room_boxes(40, 40)
-    agg, cam, ls, _ = _setup(ctx, sc)
-    out = {}
-    for pk in (0, 1):
-        img, paths = ls.guided_render(cam, 6, 8, rr_depth=3, rr_prob=0.5, seed=SEED, paths=True, sampler=sampler,
-                                      path_kernel=pk)
-        out[pk] = (img.cpu().numpy(), paths.cpu().numpy())
-    ctx.check()
-    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
-    assert out[0][0].sum() > 0
-
-
 def test_guided_rejects_bad_parameters(ctx):
     import ctypes
     from renzoku_b200 import rzk
