@@ -16,14 +16,15 @@
 // other two guided lanes its lowest: the oldest guided render takes the first guided lane
 // and its blocks are scheduled ahead of the younger renders', which only backfill SMs it
 // leaves idle, so it finishes about as fast as it would alone (the path kernel's blocks
-// are short - one thread per path - so the priorities act as SMs free up).  The gather lane keeps at most two launch groups queued on its stream (one running,
-// one behind it, so the GPU never waits for the host), each guided lane one.  Whenever a lane has room
-// the worker issues its next group from the requests not yet launched, in arrival order: on
-// the gather lane every waiting gather, oldest first, as ONE persistent batched launch of
-// at most ~2e9 evaluations (a request larger than that goes alone); on a guided lane the
-// oldest guided render (Metropolis renders only on the first guided lane: their chain pool
-// is the context's scratch).  Continuous batching: a request
-// that arrives while others run joins the lane's very next group.  A host function after a
+// are short - one thread per path - so the priorities act as SMs free up).  The gather
+// lane keeps at most two launch groups queued on its stream (one running, one behind it,
+// so the GPU never waits for the host), each guided lane one.  Whenever a lane has room
+// the worker issues its next group from the requests not yet launched, in arrival order:
+// on the gather lane every waiting gather, oldest first, as ONE persistent batched launch
+// of at most ~2e9 evaluations (a request larger than that goes alone); on a guided lane
+// the oldest guided render (Metropolis renders only on the first guided lane: their chain
+// pool is the context's scratch).  Continuous batching: a request that arrives while
+// others run joins the lane's very next group.  A host function after a
 // group's last kernel marks its requests done.  With batching off the worker issues one
 // request at a time in arrival order, with its own launches, on one stream (the plain
 // per-request baseline).  Scratch comes from the stream-ordered allocator, whose pool keeps
