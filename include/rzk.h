@@ -292,13 +292,17 @@ rzk_status rzk_gather_host(rzk_context *ctx, rzk_scene *scene, const rzk_receive
  * For callers that cannot let the library call cudaMalloc - their device memory is owned
  * by another framework's allocator or held to a fixed budget, or they run a frame loop in
  * which an allocation (which can synchronise the device or fail) is not acceptable.  The
- * scratch (a work counter, per-VPL-chunk partial sums and, when it fits, the spatially
- * ordered VPL copy with its sort scratch) is a fixed static device array of
- * RZK_NOALLOC_SCRATCH_BYTES (16 MiB) that every GPU loading the library holds until the
- * process exits; the call itself allocates and frees nothing.
- *   - Limit: n_recv * 12 bytes (rounded up to 256) must fit in the array minus 256 bytes
- *     (about 1.39 million receivers); larger requests return RZK_ERR_CAPACITY before any
- *     device work.
+ * scratch (a work counter, the spatially ordered VPL copy with its sort scratch when it
+ * fits, and the per-VPL-chunk partial sums of one band of receivers) is a fixed static
+ * device array of RZK_NOALLOC_SCRATCH_BYTES (16 MiB) that every GPU loading the library
+ * holds until the process exits; the call itself allocates and frees nothing.
+ *   - Bands: the receivers are gathered in bands of whole 8 x 4 tile rows (4 image rows;
+ *     32 receivers when image_width is 0), one after another on `stream`, each band as
+ *     large as the array allows, so any number of receivers is served.
+ *   - Limit: one band's partial sums with one chunk - min(4 * image_width, n_recv)
+ *     receivers x 12 bytes (32 x 12 without an image width) - must fit in the array
+ *     minus 256 bytes (image rows of up to ~349,000 pixels); otherwise RZK_ERR_CAPACITY
+ *     before any device work.
  *   - The current device must be the scene's context's device (else RZK_ERR_INVALID).
  *   - The first call on a device looks up the array's device address there (once per
  *     device, with that device current); make that first call before any stream capture.
@@ -306,9 +310,11 @@ rzk_status rzk_gather_host(rzk_context *ctx, rzk_scene *scene, const rzk_receive
  *     clears what it uses first): calls whose work overlaps on the GPU (other streams,
  *     other host threads) race and must be serialised by the caller.
  *   - Result: rzk_gather's chunking (at most 32 chunks of >= 128 VPLs, the VPLs in the
- *     Hilbert order) wherever its partial sums and the ordered copy fit - then the image is
- *     rzk_gather's bit for bit; otherwise fewer chunks, or the caller's VPL order, change
- *     only the float summation order.
+ *     Hilbert order) wherever the ordered copy fits beside the smallest band's partial
+ *     sums (about 130,000 VPLs for rows of up to 1,024 pixels) - then the image is
+ *     rzk_gather's bit for bit, whatever the bands; otherwise the caller's VPL order (and,
+ *     for rows too wide for 32 chunks, fewer chunks) change only the float summation
+ *     order.
  *   - Like every kernel of the library it reports a bounded wait that gave up in the
  *     context's error word, not in its return value: check rzk_context_check on the
  *     scene's context after the stream has run the call. */

@@ -254,12 +254,14 @@ __device__ __forceinline__ bool packet_visible_near(const DevScene &s, const Ray
     // every lane takes part in the vote (the cache tests above are per lane)
     alive = alive && !occluded;
     if (!__any_sync(kFull, alive)) return act && !occluded;
-    // lanes whose root test failed cannot reach any triangle below it: they stay visible
-    int top = 0;
-    stk[0] = a;
+    // lanes whose root test failed cannot reach any triangle below it: they stay visible.
+    // The warp descends straight into the child it visits next (the nearer one where both
+    // are entered) and pushes only the other: the visit order of a push-both stack, without
+    // a shared-memory store and load on the step's dependency chain.
+    int top = -1;
+    int c = a;
     bool overflow = false;
-    while (top >= 0) {
-        const int c = stk[top--];
+    for (;;) {
         const float4 *pn = s.trav + 2 * (c + 1);
         const float4 l0 = __ldg(pn), l1 = __ldg(pn + 1), r0 = __ldg(pn + 2), r1 = __ldg(pn + 3);
         const int al = __float_as_int(l0.w), ar = __float_as_int(r0.w);
@@ -285,19 +287,22 @@ __device__ __forceinline__ bool packet_visible_near(const DevScene &s, const Ray
         alive = alive && !occluded;
         const bool pl = al >= 0 && __any_sync(kFull, hl && alive);
         const bool pr = ar >= 0 && __any_sync(kFull, hr && alive);
+        if (!__any_sync(kFull, alive)) break;
         if (pl && pr) {
-            // visit the child most live lanes enter first: push it last
+            // visit the child most live lanes enter first; the other waits on the stack
             unsigned left_first = __ballot_sync(kFull, alive && hl && hr && tl <= tr);
             unsigned right_first = __ballot_sync(kFull, alive && hl && hr && tr < tl);
-            int first = __popc(left_first) >= __popc(right_first) ? al : ar;
-            int second = first == al ? ar : al;
-            if (top < STACK_CAP - 2) { stk[++top] = second; stk[++top] = first; } else overflow = true;
+            const int first = __popc(left_first) >= __popc(right_first) ? al : ar;
+            if (top < STACK_CAP - 1) stk[++top] = first == al ? ar : al; else overflow = true;
+            c = first;
         } else if (pl) {
-            if (top < STACK_CAP - 1) stk[++top] = al; else overflow = true;
+            c = al;
         } else if (pr) {
-            if (top < STACK_CAP - 1) stk[++top] = ar; else overflow = true;
+            c = ar;
+        } else {
+            if (top < 0) break;
+            c = stk[top--];
         }
-        if (!__any_sync(kFull, alive)) break;
     }
     if (overflow && s.err) atomicOr(s.err, ERR_STACK);
     return act && !occluded;

@@ -123,15 +123,44 @@ def test_noalloc_allocates_nothing(ctx, scene):
     assert torch.cuda.mem_get_info()[0] == before
 
 
+def test_noalloc_bands_match_gather(ctx):
+    """Requests whose 32 chunks of partial sums do not fit in the array at once are
+    gathered in bands of whole tile rows (4 image rows, or 32 receivers without an image
+    width): the image is still rzk_gather's, bit for bit."""
+    import torch
+    from renzoku_b200 import rzk
+    w, h = 1024, 160   # 163,840 receivers: 32 chunks of partial sums need 63 MB, ~4 bands
+    sc = sg.room_objects(300, w, h, seed_geo=51, seed_mat=52)
+    agg = rzk.AggregateCuda(ctx, sc)
+    cam = rzk.Camera(sc.camera)
+    recv = agg.primary(cam)
+    vt, n = rzk.VplGeneratorCuda(agg).spawn(53, 3000, 4)
+    assert n >= 32 * 128   # rzk_gather's full 32 chunks
+    ev = rzk.VirtualPointLightCuda(agg, rzk.CLAMP_RADIANCE, 0.05)
+    lib = rzk.load()
+    for width in (w, 0):
+        ref = ev.gather(recv, cam.n_pixels, vt, n, scale=1.0 / 3000, image_width=width).cpu().numpy()
+        assert float(np.abs(ref).sum()) > 0
+        out = torch.full((cam.n_pixels, 3), float("nan"), dtype=torch.float32, device="cuda")
+        st = _noalloc(lib, agg, recv, cam.n_pixels, width, vt, n, rzk.CLAMP_RADIANCE, 0.05, 1.0 / 3000, out)
+        assert st == rzk.OK, lib.rzk_status_string(st)
+        got = out.cpu().numpy()
+        assert np.array_equal(got, ref), (width, np.abs(got - ref).max())
+    ctx.check()
+
+
 def test_noalloc_rejects_oversized_request(ctx):
+    """The smallest band - 4 image rows - must fit with one chunk: a 2,000,000-pixel row
+    (24 MB of partial sums) is refused before any device work."""
     import torch
     from renzoku_b200 import rzk
     sc = sg.room_boxes(8, 8)
     agg = rzk.AggregateCuda(ctx, sc)
     lib = rzk.load()
-    too_many = (SCRATCH_BYTES - 256) // 12 + 1
+    row = 2_000_000
+    assert 12 * row > SCRATCH_BYTES - 256
     dummy = torch.zeros(256, dtype=torch.uint8, device="cuda")
-    st = lib.rzk_gather_noalloc(agg.h, ctypes.c_void_p(dummy.data_ptr()), too_many, 0,
+    st = lib.rzk_gather_noalloc(agg.h, ctypes.c_void_p(dummy.data_ptr()), row, row,
                                 ctypes.c_void_p(dummy.data_ptr()), 1, rzk.CLAMP_RADIANCE, 0.05, 1.0,
                                 ctypes.c_void_p(dummy.data_ptr()), rzk._stream_ptr())
     assert st == rzk.ERR_CAPACITY
