@@ -40,14 +40,14 @@ TAU_PAIRS = 65536
 # DRAM bytes (read + write) of one full gather launch of this workload, from the one-pass
 # capture `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum --clock-control none
 # -k regex:gather_persistent -s 3 -c 1 python bench.py --steps 1 --warmup 3 --skip-cpu
-# --serve-duration 0` (36.48 MB read, 55.29 MB written; the writes are the per-chunk partial
+# --serve-duration 0` (35.36 MB read, 53.50 MB written; the writes are the per-chunk partial
 # sums), recorded in profiles/.
-TRAFFIC_BYTES_PER_LAUNCH = (36.48 + 55.29) * 1e6
+TRAFFIC_BYTES_PER_LAUNCH = (35.36 + 53.50) * 1e6
 # Warp instructions of one full gather launch of this workload (smsp__inst_executed.sum from
 # the same one-pass capture, recorded in profiles/): the gather is instruction-issue bound
 # (HBM idle, its ~34 MB working set in L2), so the roofline compares the issue rate it
 # reaches with the SMs' peak of one warp instruction per scheduler per cycle.
-INST_PER_LAUNCH = 94289616557
+INST_PER_LAUNCH = 90973756923
 # The same for the secondary workloads' dominant kernels (one full launch each, same capture
 # recipe; see profiles/): LightSlice's and MRCS's tracing passes and the guided path kernel.
 LS_VIS_INST = 8180280706
@@ -383,8 +383,8 @@ def run_ours(args):
     e2e_s = max_over_ranks(pg, (time.perf_counter() - t0) / e2e_steps, "cuda")
     img_ok = bool(torch.isfinite(img_h).all()) and float(img_h.sum()) > 0
 
-    # the allocation-free entry point on the same workload (its 16 MiB static array holds
-    # the partial sums of one band of 64 image rows at a time: 8 gather launches per image)
+    # the allocation-free entry point on the same workload (its 16 MiB static array holds a
+    # chunk ring of ~1,000 tiles beside the ordered VPL copy; rzk_gather's ring has 8,192)
     out_na = torch.empty_like(out)
 
     def noalloc_step():
@@ -408,8 +408,7 @@ def run_ours(args):
     noalloc = {"value": evals_step / na_s, "unit": "evals/s", "ms_per_step": 1e3 * na_s,
                "rel_l2_vs_default": float((out_na - out).norm() / out.norm()),
                "bit_equal_to_default": bool(torch.equal(out_na, out)),
-               "note": "rzk_gather_noalloc on the same inputs; scratch in its fixed 16 MiB device array, "
-                       "receivers in bands of whole tile rows"}
+               "note": "rzk_gather_noalloc on the same inputs; scratch in its fixed 16 MiB device array"}
 
     line = None
     if rank == 0:

@@ -293,16 +293,12 @@ rzk_status rzk_gather_host(rzk_context *ctx, rzk_scene *scene, const rzk_receive
  * by another framework's allocator or held to a fixed budget, or they run a frame loop in
  * which an allocation (which can synchronise the device or fail) is not acceptable.  The
  * scratch (a work counter, the spatially ordered VPL copy with its sort scratch when it
- * fits, and the per-VPL-chunk partial sums of one band of receivers) is a fixed static
- * device array of RZK_NOALLOC_SCRATCH_BYTES (16 MiB) that every GPU loading the library
- * holds until the process exits; the call itself allocates and frees nothing.
- *   - Bands: the receivers are gathered in bands of whole 8 x 4 tile rows (4 image rows;
- *     32 receivers when image_width is 0), one after another on `stream`, each band as
- *     large as the array allows, so any number of receivers is served.
- *   - Limit: one band's partial sums with one chunk - min(4 * image_width, n_recv)
- *     receivers x 12 bytes (32 x 12 without an image width) - must fit in the array
- *     minus 256 bytes (image rows of up to ~349,000 pixels); otherwise RZK_ERR_CAPACITY
- *     before any device work.
+ * fits, and the chunk ring in which the gather sums each 8 x 4 tile's VPL chunks as soon
+ * as the tile's last chunk is done) is a fixed static device array of
+ * RZK_NOALLOC_SCRATCH_BYTES (16 MiB) that every GPU loading the library holds until the
+ * process exits; the call itself allocates and frees nothing.
+ *   - Size: the array holds the chunk sums of a window of tiles (about 1,000 tiles at 32
+ *     chunks), not of the image, so any number of receivers is served in one launch.
  *   - The current device must be the scene's context's device (else RZK_ERR_INVALID).
  *   - The first call on a device looks up the array's device address there (once per
  *     device, with that device current); make that first call before any stream capture.
@@ -310,14 +306,13 @@ rzk_status rzk_gather_host(rzk_context *ctx, rzk_scene *scene, const rzk_receive
  *     clears what it uses first): calls whose work overlaps on the GPU (other streams,
  *     other host threads) race and must be serialised by the caller.
  *   - Result: rzk_gather's chunking (at most 32 chunks of >= 128 VPLs, the VPLs in the
- *     Hilbert order) wherever the ordered copy fits beside the smallest band's partial
- *     sums (about 130,000 VPLs for rows of up to 1,024 pixels) - then the image is
- *     rzk_gather's bit for bit, whatever the bands; otherwise the caller's VPL order (and,
- *     for rows too wide for 32 chunks, fewer chunks) change only the float summation
- *     order.
+ *     Hilbert order) wherever the ordered copy leaves room for a ring of 512 tiles (up to
+ *     about 90,000 VPLs) - then the image is rzk_gather's bit for bit; beyond that the
+ *     caller's VPL order changes only the float summation order.
  *   - Like every kernel of the library it reports a bounded wait that gave up in the
  *     context's error word, not in its return value: check rzk_context_check on the
- *     scene's context after the stream has run the call. */
+ *     scene's context after the stream has run the call (the image is undefined after a
+ *     reported error). */
 rzk_status rzk_gather_noalloc(rzk_scene *scene, const rzk_receiver *d_recv, int n_recv,
                               int image_width, const rzk_vpl *d_vpls, int n_vpl, int clamp_mode,
                               float tau, float scale, float *d_rgb, void *stream);

@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) batch_gather_kernel(const __
         const int wt = local / jb.n_chunks;   // tile-major, as gather_persistent_kernel
         const int chunk = local - wt * jb.n_chunks;
         if (!gather_item<TILE, TW>(jb.s, jb.recv, jb.n_recv, jb.img_w, jb.vpls, jb.n_vpl, chunk, wt,
-                                   jb.chunk_len, jb.mode, jb.tau, jb.partial, ws, lane))
+                                   jb.chunk_len, jb.mode, jb.tau, ws, lane, PlaneSink{jb.partial, jb.n_recv, chunk}))
             break;
     }
 }

@@ -364,13 +364,98 @@ __global__ void __launch_bounds__(WARPS * 32) gather_packet_kernel(DevScene s, c
 // trace their shadow rays as a packet, nearer child first by majority; the full BRDF
 // values and the clamp are evaluated only for the lanes that stay visible (about 80% of
 // traced shadow rays are occluded on the scaled scene).  Each lane adds its terms in VPL
-// order; chunk partial sums are added in chunk order by reduce_chunks_kernel.
+// order; the chunk sums are added in chunk order by reduce_chunks_kernel after the launch
+// or, on fixed scratch, inside it through the chunk ring (RingSink).
 // ---------------------------------------------------------------------------------
 
-template <int WARPS, int TILE, int MINB, int TW = 8>
+// Bounded wait of lane 0 until a ring slot has finished `rnd` tiles (its previous tile has
+// been summed and the slot freed); ~4 s at most, then ERR_TIMEOUT.  Warp-uniform result.
+__device__ __forceinline__ bool ring_acquire(const ChunkRing &ring, int slot, int rnd, uint32_t *err, int lane) {
+    int ok = 1;
+    if (lane == 0) {
+        const volatile int *r = ring.round + slot;
+        if (*r != rnd) {
+            uint64_t t0, t;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+            for (uint32_t it = 0; *r != rnd; ++it) {
+                asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+                if (t - t0 > 4000000000ull || it > (1u << 26)) {
+                    if (err) atomicOr(err, ERR_TIMEOUT);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(200);
+            }
+        }
+        __threadfence();   // acquire: the previous tile's reads of the slot came first
+    }
+    return __shfl_sync(kFull, ok, 0) != 0;
+}
+
+// Sink of gather_item adding an item's sums to the chunk ring (ChunkRing): waits until the
+// slot's previous tile has been summed, writes the chunk's entry, counts it, and - in the
+// warp that writes the tile's last chunk - adds the tile's chunks in chunk order (the order
+// and operations of reduce_chunks_kernel, so the image is the same bit for bit), scales and
+// writes the pixels, then frees the slot.  `stop` is set when the slot wait gives up.
+struct RingSink {
+    ChunkRing ring;
+    int wt, chunk, n_chunks, lane;
+    float scale;
+    float *out;
+    uint32_t *err;
+    bool *stop;
+    __device__ __forceinline__ void operator()(int ri, Rgb sum, bool ok) const {
+        if (!ok) sum = crgb(0.0f, 0.0f, 0.0f);   // reported in the error word; the tile still completes
+        // the slot's previous tile (wt - slots) had every item handed out before this one,
+        // to warps that are running; they wait only on still earlier tiles, so the wait ends
+        const int slot = wt % ring.slots;
+        const int rnd = wt / ring.slots;
+        if (!ring_acquire(ring, slot, rnd, err, lane)) {
+            *stop = true;
+            return;
+        }
+        // streaming (evict-first) stores: the sums are read once, by the tile's last warp,
+        // and must not displace the traversal working set from L2
+        float *e = ring.sums + ((size_t)slot * n_chunks + chunk) * 96 + 3 * lane;
+        __stcs(e, sum.r); __stcs(e + 1, sum.g); __stcs(e + 2, sum.b);
+        __threadfence();   // release this chunk's sums before it is counted
+        __syncwarp();
+        int prev = 0;
+        if (lane == 0) prev = atomicAdd(ring.done + slot, 1);
+        prev = __shfl_sync(kFull, prev, 0);
+        if (prev != n_chunks - 1) return;
+        // the tile's last chunk; read past L1 (this SM may hold older lines of the slot)
+        __threadfence();
+        const float *b = ring.sums + (size_t)slot * n_chunks * 96 + 3 * lane;
+        float ar = __ldcg(b), ag = __ldcg(b + 1), ab = __ldcg(b + 2);
+        for (int c = 1; c < n_chunks; ++c) {
+            const float *bc = b + (size_t)c * 96;
+            ar += __ldcg(bc);
+            ag += __ldcg(bc + 1);
+            ab += __ldcg(bc + 2);
+        }
+        if (ri >= 0) {
+            out[3 * (size_t)ri] = ar * scale;
+            out[3 * (size_t)ri + 1] = ag * scale;
+            out[3 * (size_t)ri + 2] = ab * scale;
+        }
+        __syncwarp();   // every lane's reads of the slot precede its release
+        if (lane == 0) {
+            ring.done[slot] = 0;
+            __threadfence();
+            atomicExch(ring.round + slot, rnd + 1);
+        }
+    }
+};
+
+// RING = false: each item writes its chunk's plane of `partial` (n_chunks planes of n_recv x
+// 3 floats) and reduce_chunks_kernel adds the planes afterwards; RING = true: the chunk
+// ring (RingSink) sums each tile inside the launch and writes `out` (scaled by `scale`).
+template <int WARPS, int TILE, int MINB, int TW = 8, bool RING = false>
 __global__ void __launch_bounds__(WARPS * 32, MINB) gather_persistent_kernel(
     DevScene s, const rzk_receiver *recv, int n_recv, int img_w, const rzk_vpl *vpls, int n_vpl,
-    int chunk_len, int n_chunks, int n_wtiles, int *work, int mode, float tau, float *partial) {
+    int chunk_len, int n_chunks, int n_wtiles, int *work, int mode, float tau, float *partial, float scale,
+    ChunkRing ring, float *out) {
     __shared__ __align__(128) rzk_vpl tiles[WARPS][2][TILE];
     __shared__ __align__(8) uint64_t bar[WARPS][2];
     __shared__ int stacks[WARPS][STACK_CAP];
@@ -385,12 +470,21 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) gather_persistent_kernel(
         item = __shfl_sync(kFull, item, 0);
         if (item >= n_items) break;
         // tile-major: the warps in flight work on a few hundred neighbouring tiles (a compact
-        // band of ray origins) against every chunk
+        // band of ray origins) against every chunk; a tile's items are all handed out before
+        // any item of a later tile, which is what ends the ring's waits
         const int wt = item / n_chunks;
         const int chunk = item - wt * n_chunks;
-        if (!gather_item<TILE, TW>(s, recv, n_recv, img_w, vpls, n_vpl, chunk, wt, chunk_len, mode, tau, partial,
-                                   ws, lane))
-            break;
+        if constexpr (RING) {
+            bool stop = false;
+            const bool ok = gather_item<TILE, TW>(s, recv, n_recv, img_w, vpls, n_vpl, chunk, wt, chunk_len, mode,
+                                                  tau, ws, lane,
+                                                  RingSink{ring, wt, chunk, n_chunks, lane, scale, out, s.err, &stop});
+            if (!ok || stop) break;
+        } else {
+            if (!gather_item<TILE, TW>(s, recv, n_recv, img_w, vpls, n_vpl, chunk, wt, chunk_len, mode, tau, ws,
+                                       lane, PlaneSink{partial, n_recv, chunk}))
+                break;
+        }
     }
 }
 
@@ -735,7 +829,9 @@ rzk_status launch_gather(rzk_context *ctx, const DevScene &s, const float *box, 
                                            : warp_tiles<8>(n_recv, img_w);
     int chunk_len = 0;
     resolve_chunks(n_vpl, n_chunks, chunk_len);
-    size_t need = sizeof(float) * 3 * (size_t)n_recv * n_chunks;
+    // one plane of partial sums per chunk, added by reduce_chunks_kernel (the chunk ring that
+    // rzk_gather_noalloc sums in measured 1.3% slower here, where memory is not short)
+    const size_t need = sizeof(float) * 3 * (size_t)n_recv * n_chunks;
     if (need > ctx->partial_bytes) {
         if (ctx->d_partial) cudaFree(ctx->d_partial);
         ctx->d_partial = nullptr;
@@ -749,14 +845,15 @@ rzk_status launch_gather(rzk_context *ctx, const DevScene &s, const float *box, 
     if (gv.kind == 3) {
         RZK_CUDA_TRY(cudaMemsetAsync(ctx->d_work, 0, sizeof(int), st));
         const int wt = (int)wtiles;
+        const ChunkRing nr{};
         switch (variant) {
-            case 2: gather_persistent_kernel<4, 32, 1><<<persistent_grid<4, 32, 1>(ctx, 2), 128, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part); break;
-            case 1: gather_persistent_kernel<2, 32, 1><<<persistent_grid<2, 32, 1>(ctx, 1), 64, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part); break;
-            case 0: gather_persistent_kernel<4, 32, 5><<<persistent_grid<4, 32, 5>(ctx, 0), 128, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part); break;
-            case 8: gather_persistent_kernel<4, 32, 5, 4><<<persistent_grid<4, 32, 5, 4>(ctx, 8), 128, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part); break;
-            case 9: gather_persistent_kernel<4, 32, 5, 16><<<persistent_grid<4, 32, 5, 16>(ctx, 9), 128, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part); break;
-            case 10: gather_persistent_kernel<4, 32, 5, 32><<<persistent_grid<4, 32, 5, 32>(ctx, 10), 128, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part); break;
-            default: gather_persistent_kernel<4, 32, 6><<<persistent_grid<4, 32, 6>(ctx, 3), 128, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part); break;
+            case 2: gather_persistent_kernel<4, 32, 1><<<persistent_grid<4, 32, 1>(ctx, 2), 128, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part, scale, nr, out); break;
+            case 1: gather_persistent_kernel<2, 32, 1><<<persistent_grid<2, 32, 1>(ctx, 1), 64, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part, scale, nr, out); break;
+            case 0: gather_persistent_kernel<4, 32, 5><<<persistent_grid<4, 32, 5>(ctx, 0), 128, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part, scale, nr, out); break;
+            case 8: gather_persistent_kernel<4, 32, 5, 4><<<persistent_grid<4, 32, 5, 4>(ctx, 8), 128, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part, scale, nr, out); break;
+            case 9: gather_persistent_kernel<4, 32, 5, 16><<<persistent_grid<4, 32, 5, 16>(ctx, 9), 128, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part, scale, nr, out); break;
+            case 10: gather_persistent_kernel<4, 32, 5, 32><<<persistent_grid<4, 32, 5, 32>(ctx, 10), 128, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part, scale, nr, out); break;
+            default: gather_persistent_kernel<4, 32, 6><<<persistent_grid<4, 32, 6>(ctx, 3), 128, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part, scale, nr, out); break;
         }
     } else {
         int rb = gv.kind == 0 ? (n_recv + gv.warps_or_block - 1) / gv.warps_or_block
@@ -813,24 +910,24 @@ rzk_status launch_mean(rzk_context *ctx, const DevScene &s, const rzk_receiver *
     return RZK_OK;
 }
 
-// The persistent gather (4 warps, 32-VPL tiles, 5 CTAs per SM) on caller-provided scratch:
-// `partial` holds n_chunks x n_recv x 3 floats and `work` one int that the caller has
-// zeroed on `st`.  Used by the allocation-free entry point (rzk_noalloc.cu).
+// The persistent gather (4 warps, 32-VPL tiles, 5 CTAs per SM, 8 x 4 warp tiles) on
+// caller-provided scratch: a chunk ring in `ring_mem` with as many tile slots as its
+// `ring_mem_bytes` hold (up to kRingSlots; RZK_ERR_CAPACITY when not one fits) and the work
+// counter `work`, both zeroed on `st` first.  n_chunks as resolved by the caller (chunk
+// boundaries on multiples of 128 VPLs).  Used by the allocation-free entry point
+// (rzk_noalloc.cu).
 rzk_status launch_gather_scratch(const DevScene &s, const rzk_receiver *recv, int n_recv, int img_w,
                                  const rzk_vpl *vpls, int n_vpl, int mode, float tau, float scale,
-                                 float *out, int n_chunks, float *partial, int *work, cudaStream_t st) {
+                                 float *out, int n_chunks, void *ring_mem, size_t ring_mem_bytes, int *work,
+                                 cudaStream_t st) {
     if (n_recv <= 0) return RZK_OK;
-    long long wtiles;
-    if (img_w > 0) {
-        long long img_h = ((long long)n_recv + img_w - 1) / img_w;
-        wtiles = (long long)((img_w + 7) / 8) * ((img_h + 3) / 4);
-    } else {
-        wtiles = ((long long)n_recv + 31) / 32;
-    }
+    const long long wtiles = warp_tiles<8>(n_recv, img_w);
     if (n_vpl <= 0) n_chunks = 1;
     int chunk_len = n_vpl > 0 ? (n_vpl + n_chunks - 1) / n_chunks : 0;
     chunk_len = (chunk_len + 127) / 128 * 128;
     if (chunk_len > 0) n_chunks = (n_vpl + chunk_len - 1) / chunk_len;
+    const int slots = (int)std::min<long long>(wtiles, ring_slots_fitting(ring_mem_bytes, n_chunks));
+    if (slots < 1) return RZK_ERR_CAPACITY;
     // resident grid per device, computed once per device (std::call_once: concurrent first
     // calls from several host threads wait for the one computation)
     struct Grid {
@@ -847,16 +944,42 @@ rzk_status launch_gather_scratch(const DevScene &s, const rzk_receiver *recv, in
         int sms = 0, per_sm = 0;
         g.err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if (g.err == cudaSuccess)
-            g.err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gather_persistent_kernel<4, 32, 5>, 128, 0);
+            g.err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gather_persistent_kernel<4, 32, 5, 8, true>,
+                                                                  128, 0);
         g.blocks = std::max(1, sms * std::max(1, per_sm));
     });
     RZK_CUDA_TRY(g.err);
-    gather_persistent_kernel<4, 32, 5><<<g.blocks, 128, 0, st>>>(
-        s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, (int)wtiles, work, mode, tau, partial);
-    RZK_CUDA_TRY(cudaGetLastError());
-    reduce_chunks_kernel<<<(3 * n_recv + 255) / 256, 256, 0, st>>>(partial, n_recv, n_chunks, scale, out);
+    RZK_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(int), st));
+    RZK_CUDA_TRY(cudaMemsetAsync(ring_mem, 0, ring_counter_bytes(slots), st));
+    gather_persistent_kernel<4, 32, 5, 8, true><<<g.blocks, 128, 0, st>>>(
+        s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, (int)wtiles, work, mode, tau, nullptr, scale,
+        ring_at(ring_mem, slots), out);
     RZK_CUDA_TRY(cudaGetLastError());
     return RZK_OK;
+}
+
+// Chunk ring layout: [done: slots ints | round: slots ints](256-byte aligned) then the
+// sums, slots x n_chunks x 32 lanes x 3 floats.
+size_t ring_counter_bytes(int slots) { return ((size_t)2 * sizeof(int) * slots + 255) & ~(size_t)255; }
+
+size_t ring_bytes(int slots, int n_chunks) {
+    return ring_counter_bytes(slots) + sizeof(float) * 96 * (size_t)n_chunks * slots;
+}
+
+int ring_slots_fitting(size_t bytes, int n_chunks) {
+    const size_t per = sizeof(float) * 96 * (size_t)std::max(1, n_chunks) + 2 * sizeof(int);
+    long long k = (long long)std::min<size_t>(bytes / per, (size_t)kRingSlots);
+    while (k > 0 && ring_bytes((int)k, n_chunks) > bytes) --k;
+    return (int)k;
+}
+
+ChunkRing ring_at(void *base, int slots) {
+    ChunkRing r;
+    r.done = (int *)base;
+    r.round = r.done + slots;
+    r.sums = (float *)((char *)base + ring_counter_bytes(slots));
+    r.slots = slots;
+    return r;
 }
 
 }  // namespace rzk

@@ -340,14 +340,16 @@ __host__ __device__ __forceinline__ long long warp_tiles(long long n_recv, int i
     return (long long)((img_w + TW - 1) / TW) * ((img_h + 32 / TW - 1) / (32 / TW));
 }
 
-// One work item of the persistent gather: the 32 receivers of warp tile `wt` against VPL
-// chunk `chunk`; writes that chunk's partial sums.  Returns false if a bounded wait gave
-// up (reported in the error word).  The tile shape changes which receivers share a packet,
-// never a receiver's sum.
-template <int TILE, int TW = 8>
+// One work item of the persistent gathers: the 32 receivers of warp tile `wt` against VPL
+// chunk `chunk`.  Each lane hands `sink(ri, sum, ok)` its receiver's index (-1 for none)
+// and the sum of its terms over the chunk's VPLs in VPL order (zero without a receiver);
+// ok is false, and the sum incomplete, if a bounded wait gave up (reported in the error
+// word), and the item then returns false.  The tile shape changes which receivers share a
+// packet, never a receiver's sum.
+template <int TILE, int TW = 8, class Sink>
 __device__ __forceinline__ bool gather_item(const DevScene &s, const rzk_receiver *recv, int n_recv, int img_w,
                                             const rzk_vpl *vpls, int n_vpl, int chunk, int wt, int chunk_len,
-                                            int mode, float tau, float *partial, WarpStage<TILE> &ws, int lane) {
+                                            int mode, float tau, WarpStage<TILE> &ws, int lane, Sink &&sink) {
     const int ri = lane_receiver<TW>(wt, lane, n_recv, img_w);
     const int j0 = chunk * chunk_len;
     const int j1 = min(n_vpl, j0 + chunk_len);
@@ -365,12 +367,7 @@ __device__ __forceinline__ bool gather_item(const DevScene &s, const rzk_receive
     // a tile of inactive lanes, or an empty chunk, contributes nothing: no VPL stream (an
     // empty chunk must not arm a barrier phase that no wait consumes)
     if (n_tiles <= 0 || !__any_sync(kFull, active)) {
-        if (ri >= 0) {
-            // partial sums are read once by the chunk reduction: streaming stores keep them
-            // from displacing the traversal working set in L2
-            float *o = partial + 3 * ((size_t)chunk * n_recv + ri);
-            __stcs(o, 0.0f); __stcs(o + 1, 0.0f); __stcs(o + 2, 0.0f);
-        }
+        sink(ri, crgb(0.0f, 0.0f, 0.0f), true);
         return true;
     }
     Rgb sum = crgb(0.0f, 0.0f, 0.0f);
@@ -393,7 +390,10 @@ __device__ __forceinline__ bool gather_item(const DevScene &s, const rzk_receive
         }
         bool ok = mbar_wait_bounded(&ws.mb[buf], ws.uses[buf] & 1u, lane == 0 ? s.err : nullptr);
         ws.uses[buf]++;
-        if (__any_sync(kFull, !ok)) return false;
+        if (__any_sync(kFull, !ok)) {
+            sink(ri, sum, false);
+            return false;
+        }
         const rzk_vpl *tile = ws.tl[buf];
         const int cnt = min(TILE, j1 - (j0 + k * TILE));
         for (int v = 0; v < cnt; ++v) {
@@ -413,12 +413,24 @@ __device__ __forceinline__ bool gather_item(const DevScene &s, const rzk_receive
         __syncwarp();
     }
     if (lane == 0 && s.rays && n_rays) atomicAdd(s.rays, n_rays);
-    if (ri >= 0) {
-        float *o = partial + 3 * ((size_t)chunk * n_recv + ri);
-        __stcs(o, sum.r); __stcs(o + 1, sum.g); __stcs(o + 2, sum.b);
-    }
+    sink(ri, sum, true);
     return true;
 }
+
+// Sink of gather_item writing an item's partial sums to chunk `chunk`'s plane of `partial`
+// (planes of n_recv x 3 floats); nothing is written for an item whose wait gave up.
+struct PlaneSink {
+    float *partial;
+    int n_recv, chunk;
+    __device__ __forceinline__ void operator()(int ri, Rgb sum, bool ok) const {
+        if (ok && ri >= 0) {
+            // partial sums are read once by the chunk reduction: streaming stores keep them
+            // from displacing the traversal working set in L2
+            float *o = partial + 3 * ((size_t)chunk * n_recv + ri);
+            __stcs(o, sum.r); __stcs(o + 1, sum.g); __stcs(o + 2, sum.b);
+        }
+    }
+};
 
 // Visibility half of gather_item, for gathers split into a tracing pass and a summing
 // pass: the 32 receivers of warp tile `wt` (img_w as in lane_receiver) against VPLs [j0, j1); masks[j - j0] = ballot of

@@ -169,6 +169,22 @@ rzk_status launch_matrix(const DevScene &s, const rzk_receiver *recv, int n_recv
                          cudaStream_t st);
 // rzk_gather.cu: kernels one rzk_gather_cfg call launches
 int gather_launches(int n_recv, int n_vpl, int n_chunks);
+// Chunk ring of the persistent gather on fixed scratch (rzk_gather.cu, used by
+// rzk_gather_noalloc): the per-chunk sums of at most `slots` warp tiles at a time.  Tile t writes its chunks to slot t % slots once the slot
+// has finished t / slots tiles (`round`); the warp that writes a tile's last chunk (`done`)
+// adds the chunks in chunk order, writes the tile's pixels and frees the slot.  The
+// counters start at zero (one memset of ring_counter_bytes); the sums need no clearing.
+struct ChunkRing {
+    int *done;     // [slots] chunks of the slot's current tile written
+    int *round;    // [slots] tiles the slot has finished
+    float *sums;   // [slots][n_chunks][32 lanes][3]
+    int slots;
+};
+constexpr int kRingSlots = 8192;   // most slots a ring is given (96 MiB at 32 chunks)
+size_t ring_counter_bytes(int slots);
+size_t ring_bytes(int slots, int n_chunks);
+int ring_slots_fitting(size_t bytes, int n_chunks);   // slots whose ring fits in `bytes`
+ChunkRing ring_at(void *base, int slots);
 // rzk_gather.cu: make the context's scratch (d_partial) at least `bytes` long
 rzk_status ensure_scratch(rzk_context *ctx, size_t bytes);
 // rzk_batch.cu: plan a batch (validates jobs; no device work), then launch it on a partial

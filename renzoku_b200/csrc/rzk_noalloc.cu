@@ -5,9 +5,9 @@
 // loop where an allocation (which can synchronise the device and can fail mid-frame) is
 // not acceptable.  rzk_gather_noalloc serves them: its only scratch - the work counter of
 // the persistent kernel, the spatially ordered VPL copy with its sort scratch (when it
-// fits) and the per-chunk partial sums of one band of receivers at a time - lives in the
-// fixed array below, which every GPU that loads the library holds until the process exits.
-// The caller still passes the scene, the inputs and the output buffer.
+// fits) and the chunk ring in which the kernel sums each tile's chunks - lives in the fixed
+// array below, which every GPU that loads the library holds until the process exits.  The
+// caller still passes the scene, the inputs and the output buffer.
 #include "rzk_internal.cuh"
 
 #include <algorithm>
@@ -16,13 +16,14 @@
 namespace rzk {
 rzk_status launch_gather_scratch(const DevScene &s, const rzk_receiver *recv, int n_recv, int img_w,
                                  const rzk_vpl *vpls, int n_vpl, int mode, float tau, float scale,
-                                 float *out, int n_chunks, float *partial, int *work, cudaStream_t st);
+                                 float *out, int n_chunks, void *ring_mem, size_t ring_mem_bytes, int *work,
+                                 cudaStream_t st);
 }  // namespace rzk
 
 using namespace rzk;
 
 // Scratch of rzk_gather_noalloc: [work counter (256 B) | ordered VPLs | sort scratch |
-// partial sums of one band].
+// chunk ring].
 static __device__ __align__(256) unsigned char g_noalloc_scratch[RZK_NOALLOC_SCRATCH_BYTES];
 
 namespace {
@@ -51,15 +52,6 @@ extern "C" rzk_status rzk_gather_noalloc(rzk_scene *scene, const rzk_receiver *d
     if (n_recv > 0 && (!d_recv || !d_rgb || ((uintptr_t)d_recv & 15u))) return RZK_ERR_INVALID;
     if (n_vpl > 0 && (!d_vpls || ((uintptr_t)d_vpls & 15u))) return RZK_ERR_INVALID;
     if (clamp_mode < RZK_CLAMP_NONE || clamp_mode > RZK_CLAMP_RADIANCE) return RZK_ERR_INVALID;
-    // The receivers are gathered in bands of whole warp-tile rows (4 image rows, or 32
-    // receivers without an image width), one band after another on the stream, so that
-    // the partial sums of one band - not of the whole image - must fit.  The smallest band
-    // must fit with one chunk.
-    const size_t room = (size_t)RZK_NOALLOC_SCRATCH_BYTES - 256;
-    const long long unit = image_width > 0 ? 4LL * image_width : 32LL;
-    const long long min_band = std::min<long long>(unit, n_recv);
-    const size_t plane = sizeof(float) * 3;   // bytes of one receiver in one chunk's partial sums
-    if (plane * (size_t)min_band > room) return RZK_ERR_CAPACITY;
     if (n_recv == 0) return RZK_OK;
     int dev = 0;
     RZK_CUDA_TRY(cudaGetDevice(&dev));
@@ -75,33 +67,28 @@ extern "C" rzk_status rzk_gather_noalloc(rzk_scene *scene, const rzk_receiver *d
     }
     char *base = (char *)sa.ptr;
     int *work = (int *)base;
-    // rzk_gather's chunking (at most 32 chunks of at least 128 VPLs).  With more than one
-    // chunk the VPLs are first put in rzk_gather's spatial order (Hilbert-curve index of
-    // their cells, stable) when the ordered copy and its sort scratch fit beside the
-    // smallest band's partial sums: the image is then rzk_gather's bit for bit, since a
-    // receiver's sum depends only on the chunking and the VPL order, never on the band.
-    // Otherwise the caller's VPL order (and, for image rows too wide for 32 chunks, fewer
-    // chunks) change only the float summation order.
-    const int want_chunks = std::max(1, std::min(32, (n_vpl + 127) / 128));
+    const size_t room = (size_t)RZK_NOALLOC_SCRATCH_BYTES - 256;
+    // rzk_gather's chunking (at most 32 chunks of at least 128 VPLs) and chunk ring: the
+    // persistent kernel sums each 8 x 4 tile's chunks in chunk order as soon as the tile's
+    // last chunk is written, so the scratch holds the chunk sums of a window of tiles (a
+    // ring of slots), not of the image.  With more than one chunk the VPLs are first put in
+    // rzk_gather's spatial order (Hilbert-curve index of their cells, stable) when the
+    // ordered copy and its sort scratch leave room for a ring of at least 512 tiles (or all
+    // of the image's): the image is then rzk_gather's bit for bit, since a receiver's sum
+    // depends only on the chunking and the VPL order, never on the ring.  Otherwise the
+    // caller's VPL order changes only the float summation order.
+    const int n_chunks = std::max(1, std::min(32, (n_vpl + 127) / 128));
+    const long long wtiles = image_width > 0
+                                 ? (long long)((image_width + 7) / 8) *
+                                       ((((long long)n_recv + image_width - 1) / image_width + 3) / 4)
+                                 : ((long long)n_recv + 31) / 32;
     const size_t order_bytes = up256(sizeof(rzk_vpl) * (size_t)n_vpl) + order_scratch_bytes(n_vpl);
-    int n_chunks = want_chunks;
-    bool ordered = false;
-    size_t avail = room;
-    if (want_chunks > 1) {
-        if (order_bytes + plane * (size_t)want_chunks * (size_t)min_band <= room) {
-            ordered = true;
-            avail = room - order_bytes;
-        } else {
-            n_chunks = (int)std::max<size_t>(1, std::min<size_t>(want_chunks, room / (plane * (size_t)min_band)));
-        }
-    }
-    // the most whole units whose n_chunks partial planes fit (at least the smallest band,
-    // which fits by the choices above)
-    long long band = (long long)(avail / (plane * (size_t)n_chunks * (size_t)unit)) * unit;
-    band = std::max(band, min_band);
+    const bool ordered = n_chunks > 1 && order_bytes < room &&
+                         ring_slots_fitting(room - order_bytes, n_chunks) >= std::min<long long>(wtiles, 512);
+    const size_t ring_room = room - (ordered ? order_bytes : 0);
+    if (ring_slots_fitting(ring_room, n_chunks) < 1) return RZK_ERR_CAPACITY;
     cudaStream_t st = (cudaStream_t)stream;
-    // layout: [work counter | ordered VPLs + sort scratch | partial sums of one band]
-    float *partial = (float *)(base + 256 + (ordered ? order_bytes : 0));
+    // layout: [work counter | ordered VPLs + sort scratch | chunk ring]
     const rzk_vpl *vpls = d_vpls;
     if (ordered) {
         char *ob = base + 256;
@@ -111,18 +98,8 @@ extern "C" rzk_status rzk_gather_noalloc(rzk_scene *scene, const rzk_receiver *d
         RZK_TRY(order_vpls(t, ob + up256(sizeof(rzk_vpl) * (size_t)n_vpl), (rzk_vpl *)ob, st));
         vpls = (const rzk_vpl *)ob;
     }
-    for (long long r0 = 0; r0 < n_recv; r0 += band) {
-        const int nb = (int)std::min<long long>(band, n_recv - r0);
-        // the array keeps the previous band's and call's contents: the work counter must
-        // start at zero, and the partial sums are cleared so that no earlier values can
-        // reach the image even if a work item gives up (a bounded wait timing out, reported
-        // in the context's error word)
-        RZK_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(int), st));
-        RZK_CUDA_TRY(cudaMemsetAsync(partial, 0, plane * (size_t)nb * (size_t)n_chunks, st));
-        // a band starts on a warp-tile row, so its tiles are the whole image's tiles; the
-        // kernel packs chunk c's partial sums at c * nb * 12 bytes
-        RZK_TRY(launch_gather_scratch(scene->dev(), d_recv + r0, nb, image_width, vpls, n_vpl, clamp_mode, tau,
-                                      scale, d_rgb + 3 * r0, n_chunks, partial, work, st));
-    }
-    return RZK_OK;
+    // the array keeps the previous call's contents: the launcher zeroes the work counter and
+    // the ring's counters; every chunk sum is written before the tile's sum reads it
+    return launch_gather_scratch(scene->dev(), d_recv, n_recv, image_width, vpls, n_vpl, clamp_mode, tau, scale,
+                                 d_rgb, n_chunks, base + 256 + (ordered ? order_bytes : 0), ring_room, work, st);
 }

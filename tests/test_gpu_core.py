@@ -300,6 +300,7 @@ def test_gather_full_scale_variants_agree_and_match_oracle(ctx, oracle_built):
     assert np.array_equal(ref[pick], acc)
 
 
+
 def _spread3(x):
     x = x.astype(np.uint32) & np.uint32(0xFF)
     x = (x | (x << 16)) & np.uint32(0x030000FF)

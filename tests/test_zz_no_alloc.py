@@ -123,19 +123,21 @@ def test_noalloc_allocates_nothing(ctx, scene):
     assert torch.cuda.mem_get_info()[0] == before
 
 
-def test_noalloc_bands_match_gather(ctx):
-    """Requests whose 32 chunks of partial sums do not fit in the array at once are
-    gathered in bands of whole tile rows (4 image rows, or 32 receivers without an image
-    width): the image is still rzk_gather's, bit for bit."""
+def test_noalloc_ring_wraps_matches_gather(ctx):
+    """An image whose tiles outnumber the slots of the chunk ring that fit in the array
+    (163,840 receivers: 5,120 tiles, about 1,000 slots at 32 chunks) reuses every slot
+    several times: the image is still rzk_gather's, bit for bit, with and without an image
+    width."""
     import torch
     from renzoku_b200 import rzk
-    w, h = 1024, 160   # 163,840 receivers: 32 chunks of partial sums need 63 MB, ~4 bands
+    w, h = 1024, 160
     sc = sg.room_objects(300, w, h, seed_geo=51, seed_mat=52)
     agg = rzk.AggregateCuda(ctx, sc)
     cam = rzk.Camera(sc.camera)
     recv = agg.primary(cam)
     vt, n = rzk.VplGeneratorCuda(agg).spawn(53, 3000, 4)
     assert n >= 32 * 128   # rzk_gather's full 32 chunks
+    assert 5120 * 32 * 384 > SCRATCH_BYTES
     ev = rzk.VirtualPointLightCuda(agg, rzk.CLAMP_RADIANCE, 0.05)
     lib = rzk.load()
     for width in (w, 0):
@@ -149,18 +151,25 @@ def test_noalloc_bands_match_gather(ctx):
     ctx.check()
 
 
-def test_noalloc_rejects_oversized_request(ctx):
-    """The smallest band - 4 image rows - must fit with one chunk: a 2,000,000-pixel row
-    (24 MB of partial sums) is refused before any device work."""
+def test_noalloc_large_request(ctx):
+    """The array holds the chunk sums of a window of tiles, not of the image: a request of
+    2,000,000 receivers (2000 x 1000, more than the array could hold as one chunk plane)
+    runs, and matches rzk_gather bit for bit."""
     import torch
     from renzoku_b200 import rzk
-    sc = sg.room_boxes(8, 8)
+    sc = sg.room_objects(100, 2000, 1000, seed_geo=71, seed_mat=72)
     agg = rzk.AggregateCuda(ctx, sc)
+    cam = rzk.Camera(sc.camera)
+    recv = agg.primary(cam)
+    m = cam.n_pixels
+    assert 12 * m > SCRATCH_BYTES
+    vt, n = rzk.VplGeneratorCuda(agg).spawn(73, 200, 2)
+    n = min(n, 300)
+    ev = rzk.VirtualPointLightCuda(agg, rzk.CLAMP_RADIANCE, 0.05)
     lib = rzk.load()
-    row = 2_000_000
-    assert 12 * row > SCRATCH_BYTES - 256
-    dummy = torch.zeros(256, dtype=torch.uint8, device="cuda")
-    st = lib.rzk_gather_noalloc(agg.h, ctypes.c_void_p(dummy.data_ptr()), row, row,
-                                ctypes.c_void_p(dummy.data_ptr()), 1, rzk.CLAMP_RADIANCE, 0.05, 1.0,
-                                ctypes.c_void_p(dummy.data_ptr()), rzk._stream_ptr())
-    assert st == rzk.ERR_CAPACITY
+    ref = ev.gather(recv, m, vt, n, scale=1.0 / 200, image_width=2000).cpu().numpy()
+    assert float(np.abs(ref).sum()) > 0
+    out = torch.full((m, 3), float("nan"), dtype=torch.float32, device="cuda")
+    assert _noalloc(lib, agg, recv, m, 2000, vt, n, rzk.CLAMP_RADIANCE, 0.05, 1.0 / 200, out) == rzk.OK
+    assert np.array_equal(out.cpu().numpy(), ref)
+    ctx.check()
