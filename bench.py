@@ -50,9 +50,9 @@ TRAFFIC_BYTES_PER_LAUNCH = (35.36 + 53.50) * 1e6
 INST_PER_LAUNCH = 90973756923
 # The same for the secondary workloads' dominant kernels (one full launch each, same capture
 # recipe; see profiles/): LightSlice's and MRCS's tracing passes and the guided path kernel.
-LS_VIS_INST = 8180280706
-MRCS_VIS_INST = 1554548976
-GUIDED_INST = 422341967193
+LS_VIS_INST = 8043391693
+MRCS_VIS_INST = 1544638576
+GUIDED_INST = 407864986704
 
 
 def workload_config():

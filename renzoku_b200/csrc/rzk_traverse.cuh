@@ -8,11 +8,13 @@
 //
 // Closest hit visits nodes in exactly the reference's order (aggregate_bvh.cc:402-448):
 // pop, leaf -> triangle test that shrinks tmax, inner -> test left box then right box
-// with the current tmax, push the ones that pass (right is popped first).  Any-hit
+// with the current tmax, push the ones that pass (right is popped first); the loops here
+// go straight on to the entry that would be popped next instead of pushing and popping it.  Any-hit
 // (aggregate_bvh.cc:452-478) returns whether any reachable triangle passes; its answer
 // does not depend on visit order, so leaf children are tested as soon as their box
 // passes instead of being pushed.  Both keep the reference's 64-entry stack, which drops
-// pushes when full; a drop sets ERR_STACK in the scene's error word.
+// pushes when full (holding one entry fewer per level than the reference's, it fills
+// later); a drop sets ERR_STACK in the scene's error word.
 #pragma once
 
 #include "rzk_internal.cuh"
@@ -60,30 +62,38 @@ __device__ __forceinline__ bool any_hit(const DevScene &s, const Ray &r, float t
         load_tri(s, -1 - a, ta, tb, tc);
         return tri_hit<false>(ta, tb, tc, r, tmin, tmax, nullptr, nullptr, nullptr);
     }
+    // the loop continues into the child it would pop next (the right one where both are
+    // entered) and pushes only the other: the visit order of pushing both, without a stack
+    // store and load on each step's dependency chain
     stk.top = -1;
-    stk.push(a);
+    int c = a;
     bool overflow = false;
-    while (!stk.empty()) {
-        int c = stk.pop();
+    for (;;) {
         if (STATS) ts->inner++;
         const float4 *p = tree + 2 * (c + 1);
         float4 l0 = __ldg(p), l1 = __ldg(p + 1), r0 = __ldg(p + 2), r1 = __ldg(p + 3);
         bool hl = box_hit(l0, l1, r, tmin, tmax);
         bool hr = box_hit(r0, r1, r, tmin, tmax);
         int al = __float_as_int(l0.w), ar = __float_as_int(r0.w);
-        if (hl) {
-            if (al < 0) {
-                if (STATS) ts->leaf++;
-                load_tri(s, -1 - al, ta, tb, tc);
-                if (tri_hit<false>(ta, tb, tc, r, tmin, tmax, nullptr, nullptr, nullptr)) return true;
-            } else if (!stk.push(al)) overflow = true;
+        if (hl && al < 0) {
+            if (STATS) ts->leaf++;
+            load_tri(s, -1 - al, ta, tb, tc);
+            if (tri_hit<false>(ta, tb, tc, r, tmin, tmax, nullptr, nullptr, nullptr)) return true;
         }
-        if (hr) {
-            if (ar < 0) {
-                if (STATS) ts->leaf++;
-                load_tri(s, -1 - ar, ta, tb, tc);
-                if (tri_hit<false>(ta, tb, tc, r, tmin, tmax, nullptr, nullptr, nullptr)) return true;
-            } else if (!stk.push(ar)) overflow = true;
+        if (hr && ar < 0) {
+            if (STATS) ts->leaf++;
+            load_tri(s, -1 - ar, ta, tb, tc);
+            if (tri_hit<false>(ta, tb, tc, r, tmin, tmax, nullptr, nullptr, nullptr)) return true;
+        }
+        const bool gl = hl && al >= 0, gr = hr && ar >= 0;
+        if (gr) {
+            if (gl && !stk.push(al)) overflow = true;
+            c = ar;
+        } else if (gl) {
+            c = al;
+        } else {
+            if (stk.empty()) break;
+            c = stk.pop();
         }
     }
     if (overflow && s.err) atomicOr(s.err, ERR_STACK);
@@ -101,10 +111,12 @@ __device__ __forceinline__ int closest_hit(const DevScene &s, const Ray &r, floa
     int best = -1;
     float bt = RAY_TMAX, bb = 0.0f, bg = 0.0f;
     bool overflow = false;
+    // as any_hit: the loop continues into the entry it would pop next (the right child
+    // where both boxes pass, each tested with the tmax of that moment) and pushes only the
+    // other, so the nodes are visited in the reference's order
     stk.top = -1;
-    stk.push(__float_as_int(lo.w));
-    while (!stk.empty()) {
-        int c = stk.pop();
+    int c = __float_as_int(lo.w);
+    for (;;) {
         if (c < 0) {
             float4 ta, tb, tc;
             load_tri(s, -1 - c, ta, tb, tc);
@@ -114,11 +126,22 @@ __device__ __forceinline__ int closest_hit(const DevScene &s, const Ray &r, floa
                 bt = t; bb = b; bg = g;
                 best = -1 - c;
             }
+            if (stk.empty()) break;
+            c = stk.pop();
+            continue;
+        }
+        const float4 *p = s.nodes + 2 * (c + 1);
+        float4 l0 = __ldg(p), l1 = __ldg(p + 1), r0 = __ldg(p + 2), r1 = __ldg(p + 3);
+        const bool hl = box_hit(l0, l1, r, tmin, tmax);
+        const bool hr = box_hit(r0, r1, r, tmin, tmax);
+        if (hr) {
+            if (hl && !stk.push(__float_as_int(l0.w))) overflow = true;
+            c = __float_as_int(r0.w);
+        } else if (hl) {
+            c = __float_as_int(l0.w);
         } else {
-            const float4 *p = s.nodes + 2 * (c + 1);
-            float4 l0 = __ldg(p), l1 = __ldg(p + 1), r0 = __ldg(p + 2), r1 = __ldg(p + 3);
-            if (box_hit(l0, l1, r, tmin, tmax) && !stk.push(__float_as_int(l0.w))) overflow = true;
-            if (box_hit(r0, r1, r, tmin, tmax) && !stk.push(__float_as_int(r0.w))) overflow = true;
+            if (stk.empty()) break;
+            c = stk.pop();
         }
     }
     if (overflow && s.err) atomicOr(s.err, ERR_STACK);
