@@ -72,6 +72,15 @@ __device__ __forceinline__ RecvRegs load_receiver(const rzk_receiver *r) {
     return o;
 }
 
+// r with its tangent basis vectors u, v read again from the receiver record
+__device__ __forceinline__ RecvRegs reload_basis(RecvRegs r, const rzk_receiver *rec) {
+    const float4 *q = reinterpret_cast<const float4 *>(rec);
+    const float4 d = __ldg(q + 3), e = __ldg(q + 4);
+    r.uvn.u = mk(d.x, d.y, d.z);
+    r.uvn.v = mk(d.w, e.x, e.y);
+    return r;
+}
+
 __device__ __forceinline__ rzk_material load_material(const rzk_material *m) {
     const float4 *q = reinterpret_cast<const float4 *>(m);
     float4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2);
@@ -358,11 +367,9 @@ __device__ __forceinline__ bool gather_item(const DevScene &s, const rzk_receive
     RecvRegs r;
     r.p = mk(0.0f, 0.0f, 0.0f);   // lanes without a receiver still form (unused) rays
     bool active = false;
-    rzk_material rm;
     if (ri >= 0) {
         r = load_receiver(recv + ri);
         active = r.mat >= 0;
-        if (active) rm = load_material(s.mats + r.mat);
     }
     // a tile of inactive lanes, or an empty chunk, contributes nothing: no VPL stream (an
     // empty chunk must not arm a barrier phase that no wait consumes)
@@ -407,7 +414,10 @@ __device__ __forceinline__ bool gather_item(const DevScene &s, const rzk_receive
             Ray ray = make_ray(r.p, sub(pg.q, r.p));
             float tmax = len(sub(pg.q, r.p)) - s.tmin;
             if (packet_visible_near(s, ray, tmax, act, ws.stk, occ_cache, occ_cache2)) {
-                sum = cadd(sum, pair_radiance(s, r, rm, l, pg, mode, tau));
+                // the material and the receiver's tangent basis are read again here (L1 hits)
+                // rather than held in registers through the traversal
+                sum = cadd(sum, pair_radiance(s, reload_basis(r, recv + ri), load_material(s.mats + r.mat), l, pg,
+                                              mode, tau));
             }
         }
         __syncwarp();
