@@ -100,7 +100,7 @@ __global__ void batch_reduce_kernel(const __grid_constant__ JobTable t) {
 struct BatchVariant {
     int warps, tile, minb, tw;
 };
-const BatchVariant kBatchVariants[] = {{4, 32, 6, 8}, {4, 32, 5, 8}, {2, 32, 1, 8}, {4, 16, 5, 8},
+const BatchVariant kBatchVariants[] = {{4, 32, 7, 8}, {4, 32, 6, 8}, {2, 32, 1, 8}, {4, 16, 5, 8},
                                        {4, 32, 5, 4}, {4, 32, 5, 16}, {4, 32, 5, 32}};
 
 template <int WARPS, int TILE, int MINB, int TW = 8>
@@ -115,8 +115,8 @@ int batch_grid() {
 
 int grid_for(int variant) {
     switch (variant) {
-        case 0: return batch_grid<4, 32, 6>();
-        case 1: return batch_grid<4, 32, 5>();
+        case 0: return batch_grid<4, 32, 7>();
+        case 1: return batch_grid<4, 32, 6>();
         case 2: return batch_grid<2, 32, 1>();
         case 4: return batch_grid<4, 32, 5, 4>();
         case 5: return batch_grid<4, 32, 5, 16>();
@@ -263,8 +263,8 @@ rzk_status batch_plan_launch(BatchPlan *p, float *partial, void *order, int *wor
         int *w = work + k;
         if (p->orders[k].total > 0) RZK_TRY(order_vpls(p->orders[k], scratch, sorted + p->order_base[k], st));
         switch (variant) {
-            case 0: batch_gather_kernel<4, 32, 6><<<grid, 128, 0, st>>>(t, w); break;
-            case 1: batch_gather_kernel<4, 32, 5><<<grid, 128, 0, st>>>(t, w); break;
+            case 0: batch_gather_kernel<4, 32, 7><<<grid, 128, 0, st>>>(t, w); break;
+            case 1: batch_gather_kernel<4, 32, 6><<<grid, 128, 0, st>>>(t, w); break;
             case 2: batch_gather_kernel<2, 32, 1><<<grid, 64, 0, st>>>(t, w); break;
             case 4: batch_gather_kernel<4, 32, 5, 4><<<grid, 128, 0, st>>>(t, w); break;
             case 5: batch_gather_kernel<4, 32, 5, 16><<<grid, 128, 0, st>>>(t, w); break;

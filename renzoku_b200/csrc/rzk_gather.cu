@@ -760,9 +760,9 @@ static rzk_status order_gather_vpls(rzk_context *ctx, const float *box, const rz
 
 // Tile configurations compiled in; the autotuner picks one per workload.
 //   kind 3: persistent warp-packet kernel (the production path)      variants 0-3, 8-10
-//           (0 and 3 cap registers for 6 and 5 resident 4-warp CTAs per SM; 0 is the
-//           default, fastest on the scaled scene; 8-10 are variant 3 with warp tiles of
-//           4 x 8, 16 x 2 and 32 x 1 pixels instead of 8 x 4)
+//           (0 and 3 cap registers for 7 and 6 resident 4-warp CTAs per SM; 0 is the
+//           default, fastest on the scaled scene; 8-10 are the kernel at 5 CTAs per SM
+//           with warp tiles of 4 x 8, 16 x 2 and 32 x 1 pixels instead of 8 x 4)
 //   kind 1: warp-packet kernel, one CTA per receiver block            variants 4-5
 //   kind 2: warp-packet kernel on the 4-wide tree                     variant 6
 //   kind 0: per-thread block-lockstep kernel (first implementation)   variant 7
@@ -849,11 +849,11 @@ rzk_status launch_gather(rzk_context *ctx, const DevScene &s, const float *box, 
         switch (variant) {
             case 2: gather_persistent_kernel<4, 32, 1><<<persistent_grid<4, 32, 1>(ctx, 2), 128, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part, scale, nr, out); break;
             case 1: gather_persistent_kernel<2, 32, 1><<<persistent_grid<2, 32, 1>(ctx, 1), 64, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part, scale, nr, out); break;
-            case 0: gather_persistent_kernel<4, 32, 6><<<persistent_grid<4, 32, 6>(ctx, 0), 128, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part, scale, nr, out); break;
+            case 0: gather_persistent_kernel<4, 32, 7><<<persistent_grid<4, 32, 7>(ctx, 0), 128, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part, scale, nr, out); break;
             case 8: gather_persistent_kernel<4, 32, 5, 4><<<persistent_grid<4, 32, 5, 4>(ctx, 8), 128, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part, scale, nr, out); break;
             case 9: gather_persistent_kernel<4, 32, 5, 16><<<persistent_grid<4, 32, 5, 16>(ctx, 9), 128, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part, scale, nr, out); break;
             case 10: gather_persistent_kernel<4, 32, 5, 32><<<persistent_grid<4, 32, 5, 32>(ctx, 10), 128, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part, scale, nr, out); break;
-            default: gather_persistent_kernel<4, 32, 5><<<persistent_grid<4, 32, 5>(ctx, 3), 128, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part, scale, nr, out); break;
+            default: gather_persistent_kernel<4, 32, 6><<<persistent_grid<4, 32, 6>(ctx, 3), 128, 0, st>>>(s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, wt, ctx->d_work, mode, tau, part, scale, nr, out); break;
         }
     } else {
         int rb = gv.kind == 0 ? (n_recv + gv.warps_or_block - 1) / gv.warps_or_block
@@ -910,7 +910,7 @@ rzk_status launch_mean(rzk_context *ctx, const DevScene &s, const rzk_receiver *
     return RZK_OK;
 }
 
-// The persistent gather (4 warps, 32-VPL tiles, 6 CTAs per SM, 8 x 4 warp tiles) on
+// The persistent gather (4 warps, 32-VPL tiles, 7 CTAs per SM, 8 x 4 warp tiles) on
 // caller-provided scratch: a chunk ring in `ring_mem` with as many tile slots as its
 // `ring_mem_bytes` hold (up to kRingSlots; RZK_ERR_CAPACITY when not one fits) and the work
 // counter `work`, both zeroed on `st` first.  n_chunks as resolved by the caller (chunk
@@ -944,14 +944,14 @@ rzk_status launch_gather_scratch(const DevScene &s, const rzk_receiver *recv, in
         int sms = 0, per_sm = 0;
         g.err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if (g.err == cudaSuccess)
-            g.err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gather_persistent_kernel<4, 32, 6, 8, true>,
+            g.err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gather_persistent_kernel<4, 32, 7, 8, true>,
                                                                   128, 0);
         g.blocks = std::max(1, sms * std::max(1, per_sm));
     });
     RZK_CUDA_TRY(g.err);
     RZK_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(int), st));
     RZK_CUDA_TRY(cudaMemsetAsync(ring_mem, 0, ring_counter_bytes(slots), st));
-    gather_persistent_kernel<4, 32, 6, 8, true><<<g.blocks, 128, 0, st>>>(
+    gather_persistent_kernel<4, 32, 7, 8, true><<<g.blocks, 128, 0, st>>>(
         s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, (int)wtiles, work, mode, tau, nullptr, scale,
         ring_at(ring_mem, slots), out);
     RZK_CUDA_TRY(cudaGetLastError());

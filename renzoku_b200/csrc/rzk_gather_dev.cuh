@@ -414,9 +414,12 @@ __device__ __forceinline__ bool gather_item(const DevScene &s, const rzk_receive
             Ray ray = make_ray(r.p, sub(pg.q, r.p));
             float tmax = len(sub(pg.q, r.p)) - s.tmin;
             if (packet_visible_near(s, ray, tmax, act, ws.stk, occ_cache, occ_cache2)) {
-                // the material and the receiver's tangent basis are read again here (L1 hits)
+                // the pair's geometry (recomputed: the same operations on the same values),
+                // the material and the receiver's tangent basis are read or formed again here
                 // rather than held in registers through the traversal
-                sum = cadd(sum, pair_radiance(s, reload_basis(r, recv + ri), load_material(s.mats + r.mat), l, pg,
+                PairGeo pv;
+                pair_survives(r, l, pv);
+                sum = cadd(sum, pair_radiance(s, reload_basis(r, recv + ri), load_material(s.mats + r.mat), l, pv,
                                               mode, tau));
             }
         }

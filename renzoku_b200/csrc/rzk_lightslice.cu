@@ -1146,7 +1146,7 @@ int cluster_vis_grid() {
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cluster_vis_kernel<4, 32, 6>, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cluster_vis_kernel<4, 32, 7>, 128, 0);
     return std::max(1, sms * std::max(1, per_sm));
 }
 
@@ -1533,7 +1533,7 @@ rzk_status rzk_lightslice_gather(rzk_lightslice *L, const rzk_receiver *d_recv, 
         if (grid == 0) grid = cluster_vis_grid();
         const DevScene ds = L->scene->dev();
         if (v.n_items > 0)
-            cluster_vis_kernel<4, 32, 6><<<grid, 128, 0, st>>>(ds, L->d_perm.p, t, v, L->d_work.p);
+            cluster_vis_kernel<4, 32, 7><<<grid, 128, 0, st>>>(ds, L->d_perm.p, t, v, L->d_work.p);
         LS_TRY(cudaGetLastError());
         const long long threads = 32LL * t.n_items;
         cluster_shade_kernel<<<(unsigned)((threads + kShadeBlock - 1) / kShadeBlock), kShadeBlock, 0, st>>>(
