@@ -164,10 +164,9 @@ __device__ Rgb trace_path(const DevScene &s, const GuideDev &G, const PtParams &
         else if (METRO) brdf = guide_metro_sample_at(G, r, m, slice, g, wi, pdf);
         else brdf = guide_sample_at(G, r, m, slice, g, wi, pdf);
         if (!(pdf > 0.0f)) { value = radiance; break; }
-        Ray ray = make_ray(r.p, wi);
-        HitGeo h;
-        if (!trace_closest(s, ray, stk, h)) { value = radiance; break; }
-        if (h.light >= 0) { value = radiance; break; }   // no double count of direct light
+        // the vertex's MIS weight and cosine are formed before the closest-hit query (pure
+        // functions of values already known, so the same numbers), which leaves the vertex's
+        // receiver and material dead, not held in registers, through the traversal
         float other;
         if (is_brdf) {
             other = METRO ? guide_metro_pdf_at(G, r, slice, wi) : guide_pdf_at(G, r, slice, wi);
@@ -176,11 +175,17 @@ __device__ Rgb trace_path(const DevScene &s, const GuideDev &G, const PtParams &
             if (m.type != RZK_BSDF_LAMBERTIAN) rho_terms(m, rho_d, rho_s);
             other = brdf_pdf(m, r.uvn, r.wo, wi, rho_d, rho_s);
         }
+        const float weight = pdf / (pdf + other);
+        const float cosv = fabsf(dot(wi, r.ns));
+        Ray ray = make_ray(r.p, wi);
+        HitGeo h;
+        if (!trace_closest(s, ray, stk, h)) { value = radiance; break; }
+        if (h.light >= 0) { value = radiance; break; }   // no double count of direct light
         Vertex &v = vx[depth++];
         v.radiance = radiance;
         v.brdf = brdf;
-        v.weight = pdf / (pdf + other);
-        v.cos = fabsf(dot(wi, r.ns));
+        v.weight = weight;
+        v.cos = cosv;
         v.pdf = pdf;
         v.rr = rr;
         r = to_recv(h, ray);
