@@ -40,14 +40,14 @@ TAU_PAIRS = 65536
 # DRAM bytes (read + write) of one full gather launch of this workload, from the one-pass
 # capture `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum --clock-control none
 # -k regex:gather_persistent -s 3 -c 1 python bench.py --steps 1 --warmup 3 --skip-cpu
-# --serve-duration 0` (35.59 MB read, 54.46 MB written; the writes are the per-chunk partial
+# --serve-duration 0` (36.76 MB read, 55.23 MB written; the writes are the per-chunk partial
 # sums), recorded in profiles/.
-TRAFFIC_BYTES_PER_LAUNCH = (35.59 + 54.46) * 1e6
+TRAFFIC_BYTES_PER_LAUNCH = (36.76 + 55.23) * 1e6
 # Warp instructions of one full gather launch of this workload (smsp__inst_executed.sum from
 # the same one-pass capture, recorded in profiles/): the gather is instruction-issue bound
 # (HBM idle, its ~34 MB working set in L2), so the roofline compares the issue rate it
 # reaches with the SMs' peak of one warp instruction per scheduler per cycle.
-INST_PER_LAUNCH = 90946283508
+INST_PER_LAUNCH = 89574058624
 # The same for the secondary workloads' dominant kernels (one full launch each, same capture
 # recipe; see profiles/): LightSlice's and MRCS's tracing passes and the guided path kernel.
 LS_VIS_INST = 8043391693

@@ -125,21 +125,37 @@ struct PairGeo {
     Rgb power;
 };
 
+// The VPL-only facts the per-pair tests use: its power is finite (all three components),
+// and it was reached from behind its surface (a BRDF VPL whose stored incident direction
+// makes a cosine <= ZERO_EPSILON with its normal: its BRDF's early-out then fires for every
+// receiver).  The gathers form them once per VPL, one VPL per lane, instead of in every
+// lane for every VPL.
+__device__ __forceinline__ bool vpl_power_finite(const rzk_vpl &l) {
+    return isfinite(l.contrib[0]) && isfinite(l.contrib[1]) && isfinite(l.contrib[2]);
+}
+__device__ __forceinline__ bool vpl_from_behind(const rzk_vpl &l) {
+    return l.mat >= 0 && dot(ld3(l.wi), ld3(l.nn)) <= ZERO_EPSILON;
+}
+
 // Geometry of a pair and the exact-zero test of its term: returns false when either
-// BRDF's early-out makes the term exactly zero (G and the power finite).
-__device__ __forceinline__ bool pair_survives(const RecvRegs &r, const rzk_vpl &l, PairGeo &pg) {
+// BRDF's early-out makes the term exactly zero (G and the power finite).  `fin` and
+// `behind` are vpl_power_finite(l) and vpl_from_behind(l).
+__device__ __forceinline__ bool pair_survives(const RecvRegs &r, const rzk_vpl &l, PairGeo &pg, bool fin,
+                                              bool behind) {
     pg.q = ld3(l.p);
     pg.G = form_factor_abs(r.p, r.ns, pg.q, ld3(l.n));
     pg.wi = unit(sub(pg.q, r.p));
     pg.power = crgb(l.contrib[0], l.contrib[1], l.contrib[2]);
-    if (isfinite(pg.G) && finite3(pg.power)) {
+    if (isfinite(pg.G) && fin) {
         if (dot(pg.wi, r.uvn.n) <= ZERO_EPSILON || dot(r.wo, r.uvn.n) <= ZERO_EPSILON) return false;
-        if (l.mat >= 0) {
-            V3 lnn = ld3(l.nn);
-            if (dot(neg(pg.wi), lnn) <= ZERO_EPSILON || dot(ld3(l.wi), lnn) <= ZERO_EPSILON) return false;
-        }
+        if (behind) return false;
+        if (l.mat >= 0 && dot(neg(pg.wi), ld3(l.nn)) <= ZERO_EPSILON) return false;
     }
     return true;
+}
+
+__device__ __forceinline__ bool pair_survives(const RecvRegs &r, const rzk_vpl &l, PairGeo &pg) {
+    return pair_survives(r, l, pg, vpl_power_finite(l), vpl_from_behind(l));
 }
 
 // A cheaper first test that implies pair_survives' "exactly zero" answer: no division or
@@ -150,12 +166,13 @@ __device__ __forceinline__ bool pair_survives(const RecvRegs &r, const rzk_vpl &
 // the unnormalised direction d = q - p with a margin: dot(d, n) <= -4e-6 |d| puts the
 // rounded dot(unit(d), n) below -2e-6, under ZERO_EPSILON whatever the rounding of either
 // product (each within ~1e-6 of exact for unit normals).  Pairs it passes go through
-// pair_survives, so the set of surviving pairs is unchanged.
-__device__ __forceinline__ bool pair_clearly_zero(const RecvRegs &r, const rzk_vpl &l) {
+// pair_survives, so the set of surviving pairs is unchanged.  `fin` and `behind` as for
+// pair_survives.
+__device__ __forceinline__ bool pair_clearly_zero(const RecvRegs &r, const rzk_vpl &l, bool fin, bool behind) {
     const V3 d = sub(ld3(l.p), r.p);
     const float dd = dot(d, d);
     if (!(dd >= 1e-18f && dd <= 1e30f)) return false;
-    if (!(isfinite(l.contrib[0]) && isfinite(l.contrib[1]) && isfinite(l.contrib[2]))) return false;
+    if (!fin) return false;
     // G = |d1 d2| / dd^2 finite: d1 d2 finite and at most 1e30 dd^2
     const float g = dot(r.ns, d) * dot(ld3(l.n), d);
     if (!(fabsf(g) <= dd * dd * 1e30f)) return false;
@@ -163,13 +180,16 @@ __device__ __forceinline__ bool pair_clearly_zero(const RecvRegs &r, const rzk_v
     const float m2 = 1.6e-11f * dd;   // (4e-6)^2 |d|^2
     const float a = dot(d, r.uvn.n);
     if (a < 0.0f && a * a >= m2) return true;
+    if (behind) return true;
     if (l.mat >= 0) {
-        const V3 lnn = ld3(l.nn);
-        if (dot(ld3(l.wi), lnn) <= ZERO_EPSILON) return true;
-        const float b = dot(d, lnn);
+        const float b = dot(d, ld3(l.nn));
         if (b > 0.0f && b * b >= m2) return true;
     }
     return false;
+}
+
+__device__ __forceinline__ bool pair_clearly_zero(const RecvRegs &r, const rzk_vpl &l) {
+    return pair_clearly_zero(r, l, vpl_power_finite(l), vpl_from_behind(l));
 }
 
 __device__ __forceinline__ Rgb pair_radiance(const DevScene &s, const RecvRegs &r, const rzk_material &rm,
@@ -403,11 +423,17 @@ __device__ __forceinline__ bool gather_item(const DevScene &s, const rzk_receive
         }
         const rzk_vpl *tile = ws.tl[buf];
         const int cnt = min(TILE, j1 - (j0 + k * TILE));
+        // the VPL-only facts of the tile's VPLs, one VPL per lane
+        static_assert(TILE <= 32, "one VPL per lane");
+        const rzk_vpl &mine = tile[lane < cnt ? lane : 0];
+        const unsigned fin_mask = __ballot_sync(kFull, lane < cnt && vpl_power_finite(mine));
+        const unsigned behind_mask = __ballot_sync(kFull, lane < cnt && vpl_from_behind(mine));
         for (int v = 0; v < cnt; ++v) {
             const rzk_vpl &l = tile[v];
-            if (!__any_sync(kFull, active && !pair_clearly_zero(r, l))) continue;
+            const bool fin = (fin_mask >> v) & 1u, behind = (behind_mask >> v) & 1u;
+            if (!__any_sync(kFull, active && !pair_clearly_zero(r, l, fin, behind))) continue;
             PairGeo pg;
-            bool act = active && pair_survives(r, l, pg);
+            bool act = active && pair_survives(r, l, pg, fin, behind);
             const unsigned am = __ballot_sync(kFull, act);
             if (!am) continue;
             n_rays += (unsigned)__popc(am);
@@ -418,7 +444,7 @@ __device__ __forceinline__ bool gather_item(const DevScene &s, const rzk_receive
                 // the material and the receiver's tangent basis are read or formed again here
                 // rather than held in registers through the traversal
                 PairGeo pv;
-                pair_survives(r, l, pv);
+                pair_survives(r, l, pv, fin, behind);
                 sum = cadd(sum, pair_radiance(s, reload_basis(r, recv + ri), load_material(s.mats + r.mat), l, pv,
                                               mode, tau));
             }
