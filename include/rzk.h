@@ -48,6 +48,13 @@ rzk_status rzk_context_check(rzk_context *ctx, void *stream);
  * Aggregate::hit(p, q) (aggregate.cc:84-90).  One atomic add per warp work item.  Reads
  * after `stream` has run; reset != 0 also zeroes the counter on `stream`. */
 rzk_status rzk_context_rays(rzk_context *ctx, uint64_t *h_rays, int reset, void *stream);
+/* Failure-path check of the bounded waits (no reference counterpart): one warp runs the
+ * chunk ring's slot wait (rzk_gather_noalloc's persistent gather) on a slot that nothing
+ * frees, limited to timeout_ms (1..4000).  The wait gives up, sets the timeout bit of the
+ * context's error word (rzk_context_check then returns RZK_ERR_TIMEOUT) and the kernel
+ * returns; *h_acquired = 0 (1 would mean the wait wrongly succeeded).  Synchronises
+ * `stream`; the context stays usable. */
+rzk_status rzk_debug_ring_wait(rzk_context *ctx, int timeout_ms, int *h_acquired, void *stream);
 
 /* Aggregate ------------------------------------------------------------------------- */
 

@@ -108,6 +108,14 @@ rzk_status rzk_context_check(rzk_context *c, void *stream) {
     return RZK_OK;
 }
 
+rzk_status rzk_debug_ring_wait(rzk_context *c, int timeout_ms, int *h_acquired, void *stream) {
+    if (!c || !h_acquired || timeout_ms < 1 || timeout_ms > 4000) return RZK_ERR_INVALID;
+    int dev = 0;
+    RZK_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev != c->device) return RZK_ERR_INVALID;   // the context's buffers live on its device
+    return launch_ring_wait_probe(c, timeout_ms, h_acquired, as_stream(stream));
+}
+
 rzk_status rzk_context_rays(rzk_context *c, uint64_t *h_rays, int reset, void *stream) {
     if (!c || !h_rays) return RZK_ERR_INVALID;
     unsigned long long n = 0;

@@ -369,8 +369,10 @@ __global__ void __launch_bounds__(WARPS * 32) gather_packet_kernel(DevScene s, c
 // ---------------------------------------------------------------------------------
 
 // Bounded wait of lane 0 until a ring slot has finished `rnd` tiles (its previous tile has
-// been summed and the slot freed); ~4 s at most, then ERR_TIMEOUT.  Warp-uniform result.
-__device__ __forceinline__ bool ring_acquire(const ChunkRing &ring, int slot, int rnd, uint32_t *err, int lane) {
+// been summed and the slot freed); limit_ns of the GPU's global timer at most (4 s in the
+// gather), then ERR_TIMEOUT.  Warp-uniform result.
+__device__ __forceinline__ bool ring_acquire(const ChunkRing &ring, int slot, int rnd, uint32_t *err, int lane,
+                                             unsigned long long limit_ns = 4000000000ull) {
     int ok = 1;
     if (lane == 0) {
         const volatile int *r = ring.round + slot;
@@ -379,7 +381,7 @@ __device__ __forceinline__ bool ring_acquire(const ChunkRing &ring, int slot, in
             asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
             for (uint32_t it = 0; *r != rnd; ++it) {
                 asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-                if (t - t0 > 4000000000ull || it > (1u << 26)) {
+                if (t - t0 > limit_ns || it > (1u << 26)) {
                     if (err) atomicOr(err, ERR_TIMEOUT);
                     ok = 0;
                     break;
@@ -390,6 +392,15 @@ __device__ __forceinline__ bool ring_acquire(const ChunkRing &ring, int slot, in
         __threadfence();   // acquire: the previous tile's reads of the slot came first
     }
     return __shfl_sync(kFull, ok, 0) != 0;
+}
+
+// One warp runs the ring's slot wait on a slot that nothing frees (round 0, waiting for
+// round 1): the wait must give up after limit_ns, set ERR_TIMEOUT and return, leaving the
+// context usable.  *acquired = 1 if the wait (wrongly) succeeded.
+__global__ void ring_wait_probe_kernel(ChunkRing ring, uint32_t *err, unsigned long long limit_ns, int *acquired) {
+    const int lane = threadIdx.x & 31;
+    const bool ok = ring_acquire(ring, 0, 1, err, lane, limit_ns);
+    if (lane == 0) *acquired = ok ? 1 : 0;
 }
 
 // Sink of gather_item adding an item's sums to the chunk ring (ChunkRing): waits until the
@@ -955,6 +966,19 @@ rzk_status launch_gather_scratch(const DevScene &s, const rzk_receiver *recv, in
         s, recv, n_recv, img_w, vpls, n_vpl, chunk_len, n_chunks, (int)wtiles, work, mode, tau, nullptr, scale,
         ring_at(ring_mem, slots), out);
     RZK_CUDA_TRY(cudaGetLastError());
+    return RZK_OK;
+}
+
+rzk_status launch_ring_wait_probe(rzk_context *ctx, int timeout_ms, int *h_acquired, cudaStream_t st) {
+    RZK_TRY(ensure_scratch(ctx, ring_bytes(1, 1)));
+    char *base = (char *)ctx->d_partial;
+    int *acquired = (int *)(base + 64);   // inside the counters' 256 bytes, past the two counters
+    RZK_CUDA_TRY(cudaMemsetAsync(base, 0, ring_counter_bytes(1), st));
+    ring_wait_probe_kernel<<<1, 32, 0, st>>>(ring_at(base, 1), ctx->d_err, 1000000ull * (unsigned long long)timeout_ms,
+                                             acquired);
+    RZK_CUDA_TRY(cudaGetLastError());
+    RZK_CUDA_TRY(cudaMemcpyAsync(h_acquired, acquired, sizeof(int), cudaMemcpyDeviceToHost, st));
+    RZK_CUDA_TRY(cudaStreamSynchronize(st));
     return RZK_OK;
 }
 

@@ -185,6 +185,8 @@ size_t ring_counter_bytes(int slots);
 size_t ring_bytes(int slots, int n_chunks);
 int ring_slots_fitting(size_t bytes, int n_chunks);   // slots whose ring fits in `bytes`
 ChunkRing ring_at(void *base, int slots);
+// the ring's slot wait on a slot nothing frees, limited to timeout_ms (rzk_debug_ring_wait)
+rzk_status launch_ring_wait_probe(rzk_context *ctx, int timeout_ms, int *h_acquired, cudaStream_t st);
 // rzk_gather.cu: make the context's scratch (d_partial) at least `bytes` long
 rzk_status ensure_scratch(rzk_context *ctx, size_t bytes);
 // rzk_batch.cu: plan a batch (validates jobs; no device work), then launch it on a partial

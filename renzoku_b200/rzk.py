@@ -43,6 +43,7 @@ SIGNATURES = [
     ("rzk_context_destroy", I32, [P]),
     ("rzk_context_check", I32, [P, P]),
     ("rzk_context_rays", I32, [P, P, I32, P]),
+    ("rzk_debug_ring_wait", I32, [P, I32, P, P]),
     ("rzk_scene_create", I32, [P, P, P, P]),
     ("rzk_scene_destroy", I32, [P]),
     ("rzk_scene_info", I32, [P, P, P, P, P]),
