@@ -50,8 +50,8 @@ TRAFFIC_BYTES_PER_LAUNCH = (36.76 + 55.23) * 1e6
 INST_PER_LAUNCH = 89574058624
 # The same for the secondary workloads' dominant kernels (one full launch each, same capture
 # recipe; see profiles/): LightSlice's and MRCS's tracing passes and the guided path kernel.
-LS_VIS_INST = 8349364935
-MRCS_VIS_INST = 1544638576
+LS_VIS_INST = 8194992935
+MRCS_VIS_INST = 1532559557
 GUIDED_INST = 407466344613
 
 

@@ -515,10 +515,16 @@ __device__ __forceinline__ bool visibility_item(const DevScene &s, const rzk_rec
         if (__any_sync(kFull, !ok)) return false;
         const rzk_vpl *tile = ws.tl[buf];
         const int cnt = min(TILE, j1 - (j0 + k * TILE));
+        // the VPL-only facts of the tile's VPLs, one VPL per lane (as in gather_item)
+        static_assert(TILE <= 32, "one VPL per lane");
+        const rzk_vpl &mine = tile[lane < cnt ? lane : 0];
+        const unsigned fin_mask = __ballot_sync(kFull, lane < cnt && vpl_power_finite(mine));
+        const unsigned behind_mask = __ballot_sync(kFull, lane < cnt && vpl_from_behind(mine));
         for (int v = 0; v < cnt; ++v) {
             const rzk_vpl &l = tile[v];
+            const bool fin = (fin_mask >> v) & 1u, behind = (behind_mask >> v) & 1u;
             PairGeo pg;
-            bool act = active && !pair_clearly_zero(r, l) && pair_survives(r, l, pg);
+            bool act = active && !pair_clearly_zero(r, l, fin, behind) && pair_survives(r, l, pg, fin, behind);
             unsigned vis = 0u;
             const unsigned am = __ballot_sync(kFull, act);
             n_rays += (unsigned)__popc(am);
