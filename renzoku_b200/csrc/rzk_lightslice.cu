@@ -24,6 +24,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <queue>
 #include <thread>
 #include <utility>
@@ -1142,12 +1143,31 @@ rzk_status build(rzk_lightslice *L, const rzk_receiver *d_recv, const rzk_vpl *d
     return RZK_OK;
 }
 
-int cluster_vis_grid() {
-    int dev = 0, sms = 0, per_sm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cluster_vis_kernel<4, 32, 7>, 128, 0);
-    return std::max(1, sms * std::max(1, per_sm));
+// Resident grid of the persistent tracing kernel on the current device, computed once per
+// device (std::call_once: concurrent first calls from several host threads wait for the one
+// computation).
+cudaError_t cluster_vis_grid(int *blocks) {
+    struct Grid {
+        std::once_flag once;
+        int blocks = 0;
+        cudaError_t err = cudaSuccess;
+    };
+    constexpr int kMaxDevices = 64;
+    static Grid per_device[kMaxDevices];
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    Grid &g = per_device[dev];
+    std::call_once(g.once, [&g, dev] {
+        int sms = 0, per_sm = 0;
+        g.err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (g.err == cudaSuccess)
+            g.err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cluster_vis_kernel<4, 32, 7>, 128, 0);
+        g.blocks = std::max(1, sms * std::max(1, per_sm));
+    });
+    *blocks = g.blocks;
+    return g.err;
 }
 
 }  // namespace
@@ -1529,8 +1549,8 @@ rzk_status rzk_lightslice_gather(rzk_lightslice *L, const rzk_receiver *d_recv, 
         v.masks = L->d_masks.p;
         v.n_items = voff[ns];
         LS_TRY(cudaMemsetAsync(L->d_work.p, 0, sizeof(int), st));
-        static int grid = 0;   // resident grid of the persistent kernel (one device per process)
-        if (grid == 0) grid = cluster_vis_grid();
+        int grid = 0;
+        LS_TRY(cluster_vis_grid(&grid));
         const DevScene ds = L->scene->dev();
         if (v.n_items > 0)
             cluster_vis_kernel<4, 32, 7><<<grid, 128, 0, st>>>(ds, L->d_perm.p, t, v, L->d_work.p);
